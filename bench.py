@@ -1,0 +1,356 @@
+"""Benchmark of the B200 time-step backend (LCS.jl hot path).
+
+Workload (default "rc256", the plain-FP64 256^3 configuration): periodic cube
+L = 2pi, 256^3 cells, nu = 0.005 (Re = 200), seeded solenoidal spectral init
+E(k) ~ k^4 exp(-2 (k/4)^2) with u_rms = 1, rc-energy forcing with a 16-cell
+box filter (coarse 16^3, kmin 1, kmax 2, e10 0.649), HSMAC red-black-fast with
+time blocking and overlap, omega 1.7, itrmin 6, itrmax 300, exit at RMS(div)
+< 1e-8, CFL 0.3, dtmax 0.01, and 2^20 Stokes particles in 2 species
+(tau_p = 0.05, 0.5; density ratio 843; velocity = interpolated fluid velocity).
+
+A step is LCS.timestep! + LCS.evolve! over the whole grid and all particles.
+`value` is Mcell-steps/s (cells x steps / device seconds of the timed steps,
+max over ranks); particle-steps/s is reported beside it.  Every field is a
+(n+6)^3 FP64 array of 144 MB, so the inputs exceed the 126 MB L2 and no L2
+flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload rc256|lp128|lp512]
+
+--impl reference times the CPU restatement of the reference (oracle/, the
+port of LCSCPU: the reference is Julia and cannot run here) on the host's
+cores over a bounded number of steps of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lcs.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+from lcs_b200 import config as lcfg  # noqa: E402
+from lcs_b200 import inits  # noqa: E402
+
+WORKLOADS = {
+    # the plain FP64 method at 256^3 with rc-energy forcing
+    "rc256": dict(n=256, nu=0.005, forcing={"kind": "rc-energy", "params": {"kmin": 1, "kmax": 2, "energy": 0.649,
+                                                                            "coarse_size": 16}},
+                  taups=[0.05, 0.5], counts=[2 ** 19, 2 ** 19], precision="fp64"),
+    # 128^3, linear-power P = 0.5, 65,536 particles tau_p = 0.1
+    "lp128": dict(n=128, nu=0.01, forcing={"kind": "linear-power", "params": {"power": 0.5}}, taups=[0.1],
+                  counts=[65536], precision="fp64"),
+    # configs[2] at FP64 (the FP32-mixed form is not built yet)
+    "lp512": dict(n=512, nu=0.0025, forcing={"kind": "linear-power", "params": {"power": 0.5}},
+                  taups=[0.02, 0.2, 2.0], counts=[2 ** 24 // 3, 2 ** 24 // 3, 2 ** 24 - 2 * (2 ** 24 // 3)],
+                  precision="fp64"),
+}
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def make_run_config(name, seed=0):
+    w = WORKLOADS[name]
+    d = lcfg.workload(w["n"], w["nu"], w["forcing"], w["taups"], w["counts"], seed=seed, precision=w["precision"])
+    return lcfg.from_dict(d), w
+
+
+def host_inputs(rc, pinned=False):
+    """Seeded initial state on the host (optionally in pinned memory)."""
+    n = rc.dims[0]
+    p = rc.flow_init_params
+    U, V, W, P = inits.spectral_flow(n, seed=int(p.get("seed", 0)), urms=1.0, kpeak=4.0)
+    parts = []
+    for s, si in enumerate(rc.species):
+        x, y, z = inits.random_positions(si.nvalid, si.position_seed)
+        parts.append((np.full(si.nvalid, si.diam), x, y, z))
+    if pinned:
+        import torch
+
+        def pin(a):
+            t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = a
+            return t.numpy()
+
+        U, V, W, P = (pin(a) for a in (U, V, W, P))
+        parts = [tuple(pin(a) for a in sp) for sp in parts]
+    return (U, V, W, P), parts
+
+
+def load_engine(eng, rc, flow, parts):
+    eng.upload_flow(*flow)
+    for s, (d, x, y, z) in enumerate(parts):
+        zero = np.zeros_like(x)
+        eng.upload_particles(s, d, x, y, z, zero, zero, zero)
+        if rc.species[s].velocity == "interp":
+            eng.init_particle_velocity(s)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.stop = threading.Event()
+        self.th = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([v.strip() for v in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for name, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def reduce_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_baseline(rc, w, budget_s=30.0):
+    """The oracle (C restatement of the reference, OpenMP over all host cores)
+    on a bounded number of steps of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_engine import OracleEngine, load_oracle
+
+    flow, parts = host_inputs(rc)
+    eng = OracleEngine(rc.abi)
+    load_engine(eng, rc, flow, parts)
+    cores = load_oracle().lcs_oracle_threads()
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        eng.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el * (steps + 1) / steps > budget_s or steps >= 100:
+            break
+    el = time.perf_counter() - t0
+    n3 = float(np.prod(rc.dims))
+    np_tot = sum(w["counts"])
+    eng.close()
+    return {"value": n3 * steps / el / 1e6, "unit": "Mcell-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} full step(s) of the {rc.dims[0]}^3 workload ({el:.1f} s)",
+            "particle_steps_per_s": np_tot * steps / el, "seconds": el, "steps": steps}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    rc, w = make_run_config(args.workload)
+    line = None
+    if rank == 0:
+        base = cpu_baseline(rc, w, budget_s=float(os.environ.get("LCS_REFERENCE_BUDGET_S", "150")))
+        line = {"metric": "Mcell-steps/s", "value": base["value"], "unit": "Mcell-steps/s", "n_gpus": args.gpus,
+                "steps": base["steps"], "warmup": 0, "ms_per_step": base["seconds"] * 1e3 / base["steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded spectral field, uniform random particles)",
+                "config": {"workload": args.workload, "n": rc.dims[0], "particles": sum(w["counts"]),
+                           "species": len(w["counts"]), "parallelism": "replicas"},
+                "impl": "reference",
+                "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": base["value"], "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "particle_steps_per_s": base["particle_steps_per_s"]}
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    return 0
+
+
+def run_b200(args):
+    world, rank, local = dist_setup()
+    from lcs_b200 import Engine
+
+    rc, w = make_run_config(args.workload, seed=rank)
+    rc.abi.device = local if world > 1 else int(os.environ.get("LCS_DEVICE", "0"))
+    rc.abi.use_graphs = 1
+    n3 = float(np.prod(rc.dims))
+    np_tot = float(sum(w["counts"]))
+    flow, parts = host_inputs(rc, pinned=True)
+    eng = Engine(rc.abi)
+    load_engine(eng, rc, flow, parts)
+    # warm-up (also builds the step graph)
+    eng.step(args.warmup)
+    eng.synchronize()
+    launches0 = eng.launch_count()
+    barrier(world)
+    with ClockSampler(rc.abi.device) as clk:
+        logs, ms = eng.step_timed(args.steps)
+    launches = eng.launch_count() - launches0
+    barrier(world)
+    ms_max = reduce_max(ms, world)
+    value = world * n3 * args.steps / (ms_max / 1e3) / 1e6
+    pvalue = world * np_tot * args.steps / (ms_max / 1e3)
+    sweeps = [lg["couple1"]["sweeps"] + lg["couple2"]["sweeps"] for lg in logs]
+
+    # per-kernel device times from CUDA events around every launch (same stream)
+    eng.profile(True)
+    eng.profile_reset()
+    eng.step(2)
+    tot = eng.profile_totals()
+    eng.profile(False)
+    ms_fused, cnt = tot.get("hsmac_fused", (0.0, 0))
+    T = 8
+    peak, peak_kind = hbm_peak()
+    alg_bytes = 8 * T * n3  # U, V, W, P read and written once per interior cell per sweep
+    avg_ms = ms_fused / max(cnt, 1)
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9 if cnt else None
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in sorted(tot.items(), key=lambda kv: -kv[1][0])}
+
+    # end to end through the public API: pinned host state in, the per-step
+    # timestep!/evolve! calls of the Julia shim, state out
+    h2d0, d2h0 = eng.transfer_stats()
+    e2e_steps = max(1, min(args.steps, 5))
+    out_flow = [np.empty(eng.interior_shape) for _ in range(4)]
+    barrier(world)
+    t0 = time.perf_counter()
+    load_engine(eng, rc, flow, parts)
+    for _ in range(e2e_steps):
+        dt = eng.timestep()
+        eng.evolve(dt)
+    import ctypes as C
+
+    eng._check(eng.lib.lcs_download_flow(eng.handle, *[a.ctypes.data_as(C.POINTER(C.c_double)) for a in out_flow]))
+    for s in range(len(parts)):
+        eng.download_particles(s)
+    eng.synchronize()
+    e2e_s = reduce_max(time.perf_counter() - t0, world)
+    h2d1, d2h1 = eng.transfer_stats()
+    e2e_value = world * n3 * e2e_steps / e2e_s / 1e6
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(rc, w, budget_s=float(os.environ.get("LCS_CPU_BUDGET_S", "25")))
+    if rank == 0:
+        line = {
+            "metric": "Mcell-steps/s",
+            "value": value,
+            "unit": "Mcell-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded spectral field, uniform random particles)",
+            "config": {"workload": args.workload, "n": rc.dims[0], "particles": int(np_tot),
+                       "species": len(w["counts"]), "forcing": w["forcing"]["kind"], "hsmac_itrmax": 300,
+                       "hsmac_rms_div_tol": 1e-8, "l2": "inputs larger than L2 (144 MB per field)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "particle_steps_per_s": pvalue,
+            "hsmac_sweeps_per_step": statistics.mean(sweeps) if sweeps else None,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "roofline": {"kernel": "hsmac_fused", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": None, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
+            "kernels": kernels,
+            "e2e": {"value": e2e_value, "unit": "Mcell-steps/s",
+                    "h2d_bytes_per_step": (h2d1 - h2d0) / e2e_steps, "d2h_bytes_per_step": (d2h1 - d2h0) / e2e_steps,
+                    "steps": e2e_steps, "path": "upload + per-step lcs_timestep/lcs_evolve + download"},
+            "cpu_baseline": ({k: base[k] for k in ("value", "unit", "cores", "kind", "sample")} if base else None),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    barrier(world)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rc256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

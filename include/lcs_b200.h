@@ -1,0 +1,228 @@
+/*
+ * lcs_b200.h -- C ABI of the B200 time-step backend for LCS.jl.
+ *
+ * The reference plugs a backend into `LCS.simulate` by Julia dispatch on the
+ * backend type: `LCS.timestep!` (src/simulate.jl:55) and `LCS.evolve!`
+ * (src/simulate.jl:56) are the two per-step calls, and below them the stage
+ * functions `Flows.rhs!/update!/couple!/forcing!/timestep` and
+ * `Particles.boundary!/motion!/update!/timestep`.  A Julia package `LCSB200`
+ * binds the entry points below with `ccall`; everything else (config, init,
+ * stats, HDF5 I/O) stays in the reference's own Julia code on the host.
+ *
+ * Conventions
+ *  - Every call returns LCS_OK (0) or a negative LCS_E* code; the message is
+ *    available from lcs_last_error(h) (or lcs_last_error(NULL) when
+ *    lcs_create itself failed).  Nothing throws or aborts across the ABI.
+ *  - Host arrays are caller-owned, FP64, x fastest (Julia column-major, so a
+ *    Julia `Array{Float64,3}` of size (nx,ny,nz) is bit-for-bit the C array
+ *    [nz][ny][nx]); they are only read or written during the call.
+ *  - "interior" arrays hold the n^3 cells 1..n of each axis (`LCS.unhalo`,
+ *    src/config.jl:114-118); "haloed" arrays hold (n+2h)^3 cells with logical
+ *    index i in 1-h..n+h at offset i+h-1 (`@offsetviews`,
+ *    lib/offsets/src/Offsets.jl:70-73).
+ *  - A handle owns all device memory and one CUDA stream.  It is used by one
+ *    host thread at a time; distinct handles are independent.
+ *  - Stage arguments are 1 or 2 (`LCS.RKStage1/RKStage2`, src/rungekutta.jl).
+ *    Stage functions take the stage time increment `dtrk` the reference passes
+ *    them (`LCS.dtrk`, src/state.jl:37-38: dt/2 in stage 1, dt in stage 2).
+ */
+#ifndef LCS_B200_H
+#define LCS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LCS_API __attribute__((visibility("default")))
+#else
+#define LCS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LCS_ABI_VERSION 1
+#define LCS_MAX_SPECIES 16
+
+/* ---- status codes ------------------------------------------------------ */
+#define LCS_OK 0
+#define LCS_EINVAL (-1)      /* bad config or argument (reference: ArgumentError) */
+#define LCS_ENOMEM (-2)      /* device memory / pool budget exhausted */
+#define LCS_ECUDA (-3)       /* a CUDA runtime call failed */
+#define LCS_ETIMEDOUT (-4)   /* a bounded device wait gave up */
+#define LCS_ENONFINITE (-5)  /* NaN/Inf residual or dt */
+#define LCS_ESTATE (-6)      /* call out of order (e.g. evolve before upload) */
+
+/* ---- config enums (PolySerde kinds of the reference) ------------------- */
+enum lcs_mode { LCS_MODE_FLOW = 0, LCS_MODE_FLOW_PARTICLE = 1 };      /* src/config.jl:1-20 */
+enum lcs_coloring {                                                   /* lib/parallel/src/foraxes.jl */
+  LCS_COLORING_NO = 0,             /* NoColoring (:51) -- racy on a GPU, rejected */
+  LCS_COLORING_RED_BLACK = 1,      /* RedBlack (:82-88) */
+  LCS_COLORING_RED_BLACK_FAST = 2, /* RedBlackFast (:93-107) */
+  LCS_COLORING_RED_BLACK_BLOCK = 3 /* RedBlackBlock(size) (:114-136) */
+};
+enum lcs_forcing {                 /* src/flows/config.jl:100-175 */
+  LCS_FORCING_NO = 0,              /* "no" */
+  LCS_FORCING_LINEAR_POWER = 1,    /* "linear-power" ConstantPowerLF */
+  LCS_FORCING_RC_ENERGY = 2        /* "rc-energy" EnergyPreserveRCF */
+};
+enum lcs_drag { LCS_DRAG_LINEAR = 0, LCS_DRAG_NONLINEAR = 1 };        /* src/particles/config.jl:118-139 */
+enum lcs_precision {
+  LCS_PRECISION_FP64 = 0,          /* the reference's arithmetic (const FP = Float64, src/LCS.jl:20) */
+  LCS_PRECISION_FP32_MIXED = 1     /* FP32 fields; FP64 residuals, energies, positions (no reference counterpart) */
+};
+
+/* Field identifiers for lcs_field_set/get (src/flows/buffer.jl:38-58). */
+enum lcs_field {
+  LCS_FIELD_U = 0, LCS_FIELD_V = 1, LCS_FIELD_W = 2,    /* Us   (haloed) */
+  LCS_FIELD_U2 = 3, LCS_FIELD_V2 = 4, LCS_FIELD_W2 = 5, /* Us2  (haloed) */
+  LCS_FIELD_P = 6,                                      /* P    (haloed) */
+  LCS_FIELD_DUDT = 7, LCS_FIELD_DVDT = 8, LCS_FIELD_DWDT = 9 /* dUdts (interior only) */
+};
+
+/* Particle property identifiers (src/particles/buffer.jl:1-37). */
+enum lcs_prop {
+  LCS_PROP_X = 0, LCS_PROP_Y, LCS_PROP_Z,          /* xss   */
+  LCS_PROP_X2, LCS_PROP_Y2, LCS_PROP_Z2,           /* xss2  */
+  LCS_PROP_U, LCS_PROP_V, LCS_PROP_W,              /* uss   */
+  LCS_PROP_U2, LCS_PROP_V2, LCS_PROP_W2,           /* uss2  */
+  LCS_PROP_DUDT, LCS_PROP_DVDT, LCS_PROP_DWDT,     /* dudtss */
+  LCS_PROP_DIAM,                                   /* diams */
+  LCS_NPROP
+};
+
+/* One particle species (`ParticleConfig`, src/particles/config.jl:35-41,
+ * 118-139, 11-24).  Diameters are per particle and uploaded. */
+typedef struct lcs_species {
+  int64_t nvalid;        /* particles of this species on the device */
+  double gravity;        /* ParticleParams.gravity (acts on x, motion.jl:77) */
+  double density_ratio;  /* ParticleParams.density_ratio */
+  int32_t drag;          /* enum lcs_drag */
+  int32_t _pad;
+} lcs_species;
+
+/* POD mirror of `LCS.Config` restricted to what the time step reads. */
+typedef struct lcs_config {
+  int32_t abi_version;   /* = LCS_ABI_VERSION */
+  int32_t mode;          /* enum lcs_mode */
+  int32_t dims[3];       /* Grid.dims (cubic, even) */
+  int32_t halo_size;     /* Grid.halo_size (>= 3 for time blocking; >= 2 otherwise) */
+  double cfl, dtmax;     /* TimeStep */
+  double U0, L0, NU;     /* FlowParams (Re = U0*L0/NU) */
+  /* HSMAC (src/flows/config.jl:88-98) */
+  int32_t time_blocking, overlap, coloring, coloring_block;
+  double omega, epsp;
+  int32_t itrmin, itrmax;
+  /* forcing */
+  int32_t forcing;       /* enum lcs_forcing */
+  int32_t kmin, kmax, coarse_size;   /* rc-energy */
+  double power;          /* linear-power P0 */
+  double energy;         /* rc-energy e10 */
+  /* particles */
+  int32_t n_species;
+  int32_t precision;     /* enum lcs_precision */
+  lcs_species species[LCS_MAX_SPECIES];
+  int32_t device;        /* CUDA device ordinal */
+  int32_t use_graphs;    /* 1: lcs_step runs device-resident CUDA graphs */
+} lcs_config;
+
+/* Per-couple log `(; itr, div)` (src/flows/couples/hsmac.jl:128,200). */
+typedef struct lcs_couple_log { int32_t itr; int32_t sweeps; double div; } lcs_couple_log;
+
+/* The log NamedTuple of one `evolve!` (src/evolve.jl:124-145). */
+typedef struct lcs_log {
+  lcs_couple_log couple1, couple2;
+  double forcing_p;      /* (; p) of the forcing, NaN for "no" */
+  double forcing_e10;    /* (; e10) of rc-energy, NaN otherwise */
+  double dt;             /* dt used by this step */
+  double t;              /* time after the step */
+  int64_t step;          /* step after the step */
+} lcs_log;
+
+typedef struct lcs_handle lcs_handle;
+
+/* ---- lifetime ---------------------------------------------------------- */
+/* Replaces `LCS.Buffer(config, topo)` + `LCS.State` (src/buffer.jl:27-34, src/state.jl:27-35). */
+LCS_API int lcs_create(const lcs_config* cfg, lcs_handle** out);
+LCS_API void lcs_destroy(lcs_handle* h);
+LCS_API const char* lcs_last_error(const lcs_handle* h);
+/* Bytes of device memory the handle holds (the serving admission uses it). */
+LCS_API int lcs_footprint(const lcs_config* cfg, int64_t* bytes);
+
+/* ---- state transfer (host FP64 in every precision form) ---------------- */
+/* Interior U,V,W,P in, halos left for the next synchalo (src/flows/inits/init.jl). */
+LCS_API int lcs_upload_flow(lcs_handle* h, const double* U, const double* V, const double* W, const double* P);
+LCS_API int lcs_download_flow(lcs_handle* h, double* U, double* V, double* W, double* P);
+/* Whole field, interior (haloed=0) or haloed (haloed=1) layout. */
+LCS_API int lcs_field_set(lcs_handle* h, int32_t field, const double* data, int32_t haloed);
+LCS_API int lcs_field_get(lcs_handle* h, int32_t field, double* data, int32_t haloed);
+/* All valid particles of one species (src/particles/init.jl). ids may be NULL. */
+LCS_API int lcs_upload_particles(lcs_handle* h, int32_t species, int64_t n, const int64_t* ids, const double* diam,
+                         const double* x, const double* y, const double* z,
+                         const double* u, const double* v, const double* w);
+LCS_API int lcs_download_particles(lcs_handle* h, int32_t species, int64_t* ids, double* diam,
+                           double* x, double* y, double* z, double* u, double* v, double* w);
+LCS_API int lcs_prop_set(lcs_handle* h, int32_t species, int32_t prop, const double* data);
+LCS_API int lcs_prop_get(lcs_handle* h, int32_t species, int32_t prop, double* data);
+/* State (step, t) as `LCS.State` holds it. */
+LCS_API int lcs_set_state(lcs_handle* h, int64_t step, double t);
+LCS_API int lcs_get_state(lcs_handle* h, int64_t* step, double* t);
+
+/* ---- the per-step calls ------------------------------------------------ */
+/* `LCS.timestep` (src/timestep.jl:14-27): min(Flows.timestep, Particles.timestep). */
+LCS_API int lcs_timestep(lcs_handle* h, double* dt);
+/* `LCS.evolve!` (src/evolve.jl:15-146) with state.dt = dt; fills *log if non-NULL. */
+LCS_API int lcs_evolve(lcs_handle* h, double dt, lcs_log* log);
+/* nsteps x (timestep! + evolve!) with no host round trip in between;
+ * logs[nsteps] may be NULL. */
+LCS_API int lcs_step(lcs_handle* h, int32_t nsteps, lcs_log* logs);
+/* lcs_step, with the device time of the nsteps measured by CUDA events
+ * recorded on the handle's stream before the first and after the last step. */
+LCS_API int lcs_step_timed(lcs_handle* h, int32_t nsteps, lcs_log* logs, double* device_ms);
+
+/* ---- stage functions (one reference function each) -------------------- */
+/* `Topologies.synchalo!(FullHalo(r) | FaceHalo(r), fields)` single process
+ * (lib/topologies/src/halo.jl:138-159).  fields is a bitmask of 1<<lcs_field. */
+LCS_API int lcs_synchalo(lcs_handle* h, int32_t field_mask, int32_t r, int32_t full);
+/* `Flows.rhs!` (src/flows/rhs.jl:20-42) on Us_rhs(stage) -> dUdts. */
+LCS_API int lcs_flow_rhs(lcs_handle* h, int32_t stage);
+/* `Flows.update!` (src/flows/update.jl:23-54): Us_update(stage) = Us0 + dUdts*dtrk. */
+LCS_API int lcs_flow_update(lcs_handle* h, int32_t stage, double dtrk);
+/* rhs! then update! fused in one pass (dUdts is not written). */
+LCS_API int lcs_flow_rhs_update(lcs_handle* h, int32_t stage, double dtrk);
+/* `Flows.couple!(::HSMAC)` (src/flows/couples/hsmac.jl:52-75) on Us_couple(stage). */
+LCS_API int lcs_flow_couple(lcs_handle* h, int32_t stage, double dtrk, lcs_couple_log* log);
+/* `Flows.forcing!` stage 2 (src/flows/forcings/{lf,rcf}.jl) on Us; p and e10 out. */
+LCS_API int lcs_flow_forcing(lcs_handle* h, double dtrk, double* p, double* e10);
+/* `Flows.timestep` (src/flows/timestep.jl:18-65), including its FaceHalo sync. */
+LCS_API int lcs_flow_timestep(lcs_handle* h, double* dt);
+/* `Particles.timestep` (src/particles/timestep.jl:6-25) over all species. */
+LCS_API int lcs_particles_timestep(lcs_handle* h, double* dt);
+/* `Particles.boundary!` periodic part (src/particles/boundary.jl:33-120). */
+LCS_API int lcs_particles_boundary(lcs_handle* h, int32_t species, int32_t stage);
+/* `Particles.motion!` (src/particles/motion.jl:10-84). */
+LCS_API int lcs_particles_motion(lcs_handle* h, int32_t species, int32_t stage);
+/* `Particles.update!` (src/particles/update.jl:19-65). */
+LCS_API int lcs_particles_update(lcs_handle* h, int32_t species, int32_t stage, double dtrk);
+/* New init kind (no reference counterpart): particle velocity = the trilinear
+ * interpolation (src/particles/interp.jl:62-126) of the current Us at xss. */
+LCS_API int lcs_init_particle_velocity(lcs_handle* h, int32_t species);
+
+/* ---- profiling (`LCS_LOG_LEVEL=PROFILE`, src/log.jl:6-20) --------------- */
+/* When enabled, every kernel launch is bracketed by CUDA events on the
+ * handle's stream; totals are per kernel label. */
+LCS_API int lcs_profile_enable(lcs_handle* h, int32_t on);
+LCS_API int lcs_profile_reset(lcs_handle* h);
+LCS_API int lcs_profile_count(lcs_handle* h, int32_t* n);
+LCS_API int lcs_profile_entry(lcs_handle* h, int32_t i, char* name, int32_t name_cap, double* total_ms, int64_t* launches);
+/* Number of this library's kernel launches since creation (or the last reset). */
+LCS_API int lcs_launch_count(lcs_handle* h, int64_t* launches);
+/* Bytes this handle copied host->device and device->host since creation. */
+LCS_API int lcs_transfer_stats(lcs_handle* h, int64_t* h2d_bytes, int64_t* d2h_bytes);
+LCS_API int lcs_synchronize(lcs_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LCS_B200_H */

@@ -1,0 +1,1043 @@
+// lcs_engine.cuh -- host orchestration of one time-step handle.
+//
+// Engine<T> owns a single device allocation (the pool) carved into the
+// haloed fields, scratch and particle arrays, one CUDA stream, and the
+// device context.  It replays `LCS.evolve!` (src/evolve.jl:63-146) stage by
+// stage, and `lcs_step` captures whole steps into CUDA graphs whose HSMAC
+// loops are device-side WHILE nodes, so a step needs no host round trip.
+#pragma once
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lcs_b200.h"
+#include "lcs_base.h"
+#include "lcs_kernels.cuh"
+
+namespace lcs {
+
+// Bytes of the device pool for a config (every allocation the handle makes).
+template <typename T>
+struct Plan {
+  Grid g;
+  size_t off_vel[3][3], off_P, off_dU[3], off_stage, off_partials, off_ctx, off_logs, off_rcf, off_sp[LCS_MAX_SPECIES];
+  size_t bytes;
+  int64_t stage_elems, partials_cap, logs_cap;
+  int64_t rcf_coarse, rcf_hat, rcf_Ac, rcf_tw, rcf_en0, rcf_ph;
+};
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+template <typename T>
+Plan<T> make_plan(const lcs_config& c) {
+  Plan<T> p;
+  p.g = make_grid<T>(c.dims, c.halo_size);
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o = align_up(o + bytes, 256);
+    return at;
+  };
+  const size_t fb = (size_t)p.g.elems * sizeof(T);
+  for (int s = 0; s < 3; s++)
+    for (int q = 0; q < 3; q++) p.off_vel[s][q] = take(fb);
+  p.off_P = take(fb);
+  const int64_t ni = (int64_t)c.dims[0] * c.dims[1] * c.dims[2];
+  for (int q = 0; q < 3; q++) p.off_dU[q] = take((size_t)ni * sizeof(T));
+  const int64_t hs = (int64_t)(c.dims[0] + 2 * c.halo_size) * (c.dims[1] + 2 * c.halo_size) *
+                     (c.dims[2] + 2 * c.halo_size);
+  int64_t pmax = 0;
+  for (int s = 0; s < c.n_species; s++) pmax = std::max<int64_t>(pmax, c.species[s].nvalid);
+  p.stage_elems = std::max<int64_t>(hs, pmax);
+  p.off_stage = take((size_t)p.stage_elems * sizeof(double));
+  p.partials_cap = 1 << 20;
+  p.off_partials = take((size_t)p.partials_cap * sizeof(double));
+  p.off_ctx = take(sizeof(Ctx));
+  p.logs_cap = 4096;
+  p.off_logs = take((size_t)p.logs_cap * sizeof(StepLog));
+  // rc-energy buffers
+  const int cs = c.forcing == LCS_FORCING_RC_ENERGY ? c.coarse_size : 1;
+  const int km = c.forcing == LCS_FORCING_RC_ENERGY ? c.kmax : 1;
+  const int nm = (km + 1) * (2 * km + 1) * (2 * km + 1);
+  p.rcf_coarse = 3 * (int64_t)cs * cs * cs;
+  p.rcf_hat = 2 * 3 * (int64_t)nm;
+  p.rcf_Ac = p.rcf_hat;
+  p.rcf_tw = 2 * (int64_t)cs;
+  p.rcf_en0 = 16;
+  p.rcf_ph = 2 * (int64_t)(c.dims[0] + c.dims[1] + c.dims[2] + 3);
+  p.off_rcf = take((size_t)(p.rcf_coarse + p.rcf_hat + p.rcf_Ac + p.rcf_tw + p.rcf_en0 + p.rcf_ph) * sizeof(double));
+  for (int s = 0; s < c.n_species; s++) p.off_sp[s] = take((size_t)c.species[s].nvalid * (16 * sizeof(double) + 8));
+  p.bytes = o;
+  return p;
+}
+
+inline void sincospi_host(double x, double* s, double* c) {
+  // sin(pi x), cos(pi x) with exact reduction of x (Julia's cispi)
+  double r = std::fmod(x, 2.0);
+  if (r < 0) r += 2.0;
+  int neg_s = 0, neg_c = 0;
+  if (r >= 1.0) { r -= 1.0; neg_s = 1; neg_c = 1; }
+  if (r > 0.5) { r = 1.0 - r; neg_c = !neg_c; }
+  double ss, cc;
+  const double pi = 3.14159265358979323846;
+  if (r == 0.0) { ss = 0.0; cc = 1.0; }
+  else if (r == 0.5) { ss = 1.0; cc = 0.0; }
+  else if (r <= 0.25) { ss = std::sin(pi * r); cc = std::cos(pi * r); }
+  else { double t = 0.5 - r; ss = std::cos(pi * t); cc = std::sin(pi * t); }
+  *s = neg_s ? -ss : ss;
+  *c = neg_c ? -cc : cc;
+}
+
+inline int host_kcount(int k0) {
+  int c = 0;
+  for (int kz = -k0; kz <= k0; kz++)
+    for (int ky = -k0; ky <= k0; ky++)
+      for (int kx = -k0; kx <= k0; kx++) {
+        int r2 = kx * kx + ky * ky + kz * kz;
+        if ((k0 - 0.5) * (k0 - 0.5) <= r2 && r2 < (k0 + 0.5) * (k0 + 0.5)) c++;
+      }
+  return c;
+}
+
+// kset(k0) in the reference's generation order (FourierTools.jl:59-80)
+inline void host_kset(int k0, std::vector<std::array<int, 3>>& out) {
+  std::vector<std::array<int, 3>> K;
+  for (int kz = -k0; kz <= k0; kz++)
+    for (int ky = -k0; ky <= k0; ky++)
+      for (int kx = 0; kx <= k0; kx++) {
+        int r2 = kx * kx + ky * ky + kz * kz;
+        if (!((k0 - 0.5) * (k0 - 0.5) <= r2 && r2 < (k0 + 0.5) * (k0 + 0.5))) continue;
+        int sgn = 1;
+        const int k[3] = {kx, ky, kz};
+        for (int a = 0; a < 3; a++) {
+          if (k[a] > 0) { sgn = 1; break; }
+          if (k[a] < 0) { sgn = -1; break; }
+        }
+        std::array<int, 3> cc = {sgn * kx, sgn * ky, sgn * kz};
+        bool seen = false;
+        for (auto& e : K) seen |= (e == cc);
+        if (!seen) K.push_back(cc);
+      }
+  out.insert(out.end(), K.begin(), K.end());
+}
+
+template <typename T>
+class Engine : public EngineBase {
+ public:
+  lcs_config cfg;
+  Plan<T> plan;
+  Grid g;
+  cudaStream_t stream = nullptr;
+  char* pool = nullptr;
+  Ctx* dctx = nullptr;
+  StepLog* dlogs = nullptr;
+  T* P = nullptr;
+  T* dU[3] = {nullptr, nullptr, nullptr};
+  void* vel0[3][3];
+  double* stage = nullptr;
+  double* partials = nullptr;
+  double *rcf_coarse = nullptr, *rcf_hat = nullptr, *rcf_Ac = nullptr, *rcf_tw = nullptr, *rcf_en0 = nullptr;
+  double2 *ph[3] = {nullptr, nullptr, nullptr};
+  RcfModes modes;
+  SpeciesDev sp[LCS_MAX_SPECIES];
+  bool uploaded_flow = false;
+  int64_t launches = 0;
+  // profiling
+  bool prof = false;
+  struct Rec { std::string label; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> event_pool;
+  struct Tot { std::string label; double ms; int64_t n; };
+  std::vector<Tot> totals;
+  // host-pinned mirrors
+  Ctx* hctx = nullptr;
+  // graphs
+  cudaGraphExec_t step_exec = nullptr, evolve_exec = nullptr;
+  cudaGraph_t step_graph = nullptr, evolve_graph = nullptr;
+  int64_t graph_launches_per_step = 0, graph_launches_per_evolve = 0;
+
+  HsmacCoef hc;
+  RhsCoef rc;
+  DtCoef dc;
+  PartCoef pc;
+
+  ~Engine() override {
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (step_graph) cudaGraphDestroy(step_graph);
+    if (evolve_exec) cudaGraphExecDestroy(evolve_exec);
+    if (evolve_graph) cudaGraphDestroy(evolve_graph);
+    for (auto& r : recs) { event_pool.push_back(r.a); event_pool.push_back(r.b); }
+    for (auto e : event_pool) cudaEventDestroy(e);
+    if (hctx) cudaFreeHost(hctx);
+    if (pool) cudaFree(pool);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  int init(const lcs_config& c) {
+    cfg = c;
+    plan = make_plan<T>(c);
+    g = plan.g;
+    LCS_CUDA(cudaSetDevice(c.device));
+    LCS_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    cudaError_t e = cudaMalloc(&pool, plan.bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      pool = nullptr;
+      return fail(LCS_ENOMEM, "cudaMalloc of %zu bytes failed: %s", plan.bytes, cudaGetErrorString(e));
+    }
+    LCS_CUDA(cudaMallocHost(&hctx, sizeof(Ctx)));
+    for (int s = 0; s < 3; s++)
+      for (int q = 0; q < 3; q++) vel0[s][q] = pool + plan.off_vel[s][q];
+    P = (T*)(pool + plan.off_P);
+    for (int q = 0; q < 3; q++) dU[q] = (T*)(pool + plan.off_dU[q]);
+    stage = (double*)(pool + plan.off_stage);
+    partials = (double*)(pool + plan.off_partials);
+    dctx = (Ctx*)(pool + plan.off_ctx);
+    dlogs = (StepLog*)(pool + plan.off_logs);
+    double* r = (double*)(pool + plan.off_rcf);
+    rcf_coarse = r; r += plan.rcf_coarse;
+    rcf_hat = r; r += plan.rcf_hat;
+    rcf_Ac = r; r += plan.rcf_Ac;
+    rcf_tw = r; r += plan.rcf_tw;
+    rcf_en0 = r; r += plan.rcf_en0;
+    ph[0] = (double2*)r;
+    ph[1] = ph[0] + (c.dims[0] + 1);
+    ph[2] = ph[1] + (c.dims[1] + 1);
+    // zero every field (halos included) so no stale bits are ever read
+    LCS_CUDA(cudaMemsetAsync(pool, 0, plan.off_stage, stream));
+    Ctx h0;
+    memset(&h0, 0, sizeof h0);
+    for (int s = 0; s < 3; s++)
+      for (int q = 0; q < 3; q++) h0.vel[s][q] = vel0[s][q];
+    h0.dt_particles = c.dtmax;
+    h0.cur.p = NAN;
+    h0.cur.e10 = NAN;
+    *hctx = h0;
+    LCS_CUDA(cudaMemcpyAsync(dctx, hctx, sizeof(Ctx), cudaMemcpyHostToDevice, stream));
+    for (int s = 0; s < c.n_species; s++) {
+      char* b = pool + plan.off_sp[s];
+      sp[s].n = c.species[s].nvalid;
+      for (int q = 0; q < 16; q++) sp[s].p[q] = (double*)b + (size_t)q * sp[s].n;
+      sp[s].gravity = c.species[s].gravity;
+      sp[s].density_ratio = c.species[s].density_ratio;
+      sp[s].drag = c.species[s].drag;
+      LCS_CUDA(cudaMemsetAsync(b, 0, (size_t)sp[s].n * (16 * sizeof(double) + 8), stream));
+    }
+    // coefficients
+    const double dx = kDomainLength / c.dims[0], dy = kDomainLength / c.dims[1], dz = kDomainLength / c.dims[2];
+    const double Re = c.U0 * c.L0 / c.NU;
+    rc.dxi = 1.0 / dx; rc.dyi = 1.0 / dy; rc.dzi = 1.0 / dz; rc.Rei = 1.0 / Re;
+    hc.dxi = rc.dxi; hc.dyi = rc.dyi; hc.dzi = rc.dzi;
+    hc.dl = 1.0 / (2.0 * (hc.dxi * hc.dxi + hc.dyi * hc.dyi + hc.dzi * hc.dzi));
+    hc.omega = c.omega;
+    hc.dxmin = std::fmin(dx, std::fmin(dy, dz));
+    hc.epsp = c.epsp;
+    hc.count = (double)((int64_t)(c.dims[0] + 1) * (c.dims[1] + 1) * (c.dims[2] + 1));
+    hc.itrmin = c.itrmin;
+    hc.itrmax = c.itrmax;
+    hc.coloring = c.coloring;
+    dc.cfl = c.cfl; dc.dtmax = c.dtmax; dc.dx = dx; dc.dy = dy; dc.dz = dz; dc.Re = Re;
+    dc.with_particles = c.mode == LCS_MODE_FLOW_PARTICLE && c.n_species > 0;
+    pc.dx = dx; pc.dy = dy; pc.dz = dz; pc.Re = Re;
+    if (c.forcing == LCS_FORCING_RC_ENERGY) LCS_TRY(init_rcf());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+
+  int init_rcf() {
+    const int cs = cfg.coarse_size;
+    std::vector<double> tw(2 * cs);
+    for (int x = 0; x < cs; x++) sincospi_host(-2.0 * x / cs, &tw[2 * x + 1], &tw[2 * x]);
+    LCS_TRY(copy(rcf_tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<double> en0(16, 0.0);
+    for (int k0 = cfg.kmin; k0 <= cfg.kmax; k0++) {  // enespe0 (rcf.jl:187-191)
+      const double c1 = host_kcount(1), ck = host_kcount(k0);
+      const double a = k0 + 0.5, b = k0 - 0.5;
+      en0[k0 - cfg.kmin] = cfg.energy * std::pow((double)k0, -5.0 / 3.0) * (1.5 * 1.5 * 1.5 - 0.5 * 0.5 * 0.5) /
+                           (a * a * a - b * b * b) * ck / c1;
+    }
+    LCS_TRY(copy(rcf_en0, en0.data(), 16 * sizeof(double), cudaMemcpyHostToDevice));
+    const double phi = (double)(cfg.dims[0] / cs) / 2.0;  // phase_shift (flows/config.jl:149)
+    for (int a = 0; a < 3; a++) {
+      std::vector<double> t(2 * (cfg.dims[a] + 1), 0.0);
+      for (int i = 1; i <= cfg.dims[a]; i++) sincospi_host(2.0 * (i - phi) * (1.0 / cfg.dims[a]), &t[2 * i + 1], &t[2 * i]);
+      LCS_TRY(copy(ph[a], t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    std::vector<std::array<int, 3>> ks;
+    memset(&modes, 0, sizeof modes);
+    modes.nshell = cfg.kmax - cfg.kmin + 1;
+    for (int K = cfg.kmin; K <= cfg.kmax; K++) {
+      modes.kofs[K - cfg.kmin] = (int)ks.size();
+      host_kset(K, ks);
+    }
+    modes.kofs[modes.nshell] = (int)ks.size();
+    if (ks.size() > 128) return fail(LCS_EINVAL, "rc-energy kset too large (%zu modes)", ks.size());
+    modes.n = (int)ks.size();
+    for (size_t q = 0; q < ks.size(); q++)
+      for (int a = 0; a < 3; a++) modes.k[q][a] = (signed char)ks[q][a];
+    return LCS_OK;
+  }
+
+  // ---------------------------------------------------------------- launch
+  cudaEvent_t get_event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  bool capturing = false;
+  template <typename K, typename... A>
+  int launch(const char* label, K kernel, dim3 grid, dim3 block, size_t smem, A... args) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (prof && !capturing) {
+      a = get_event();
+      b = get_event();
+      cudaEventRecord(a, stream);
+    }
+    kernel<<<grid, block, smem, stream>>>(args...);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(LCS_ECUDA, "launch %s: %s", label, cudaGetErrorString(e));
+    if (a) {
+      cudaEventRecord(b, stream);
+      recs.push_back({label, a, b});
+    }
+    launches++;
+    return LCS_OK;
+  }
+  int collect_profile() {
+    if (recs.empty()) return LCS_OK;
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    for (auto& r : recs) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      bool found = false;
+      for (auto& t : totals)
+        if (t.label == r.label) { t.ms += ms; t.n++; found = true; break; }
+      if (!found) totals.push_back({r.label, (double)ms, 1});
+      event_pool.push_back(r.a);
+      event_pool.push_back(r.b);
+    }
+    recs.clear();
+    return LCS_OK;
+  }
+
+  static unsigned int blocks_for(int64_t n, int bs, int64_t cap = 148 * 16) {
+    int64_t b = (n + bs - 1) / bs;
+    return (unsigned int)std::max<int64_t>(1, std::min<int64_t>(b, cap));
+  }
+
+  // host<->device copies, counted for lcs_transfer_stats
+  int64_t h2d_bytes = 0, d2h_bytes = 0;
+  int copy(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    if (bytes == 0) return LCS_OK;
+    LCS_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, stream));
+    if (kind == cudaMemcpyHostToDevice) h2d_bytes += (int64_t)bytes;
+    if (kind == cudaMemcpyDeviceToHost) d2h_bytes += (int64_t)bytes;
+    return LCS_OK;
+  }
+
+  // ------------------------------------------------------------ primitives
+  int fill(int set, bool withP, int r, int full) {
+    FillArgs fa;
+    memset(&fa, 0, sizeof fa);
+    fa.nf = 0;
+    if (set >= 0)
+      for (int q = 0; q < 3; q++) { fa.set[fa.nf] = set; fa.comp[fa.nf] = q; fa.ptr[fa.nf] = nullptr; fa.nf++; }
+    if (withP) { fa.set[fa.nf] = -1; fa.comp[fa.nf] = 0; fa.ptr[fa.nf] = P; fa.nf++; }
+    const int64_t total = fill_count(g, r, full);
+    return launch("synchalo", k_fill_halo<T>, dim3(blocks_for(total, 256)), dim3(256), 0, (const Ctx*)dctx, g, fa, r,
+                  full, total);
+  }
+
+  int set_stage_dt(int stage) { return launch("stage_dt", k_set_stage_dt, dim3(1), dim3(1), 0, dctx, stage); }
+  int set_scalar(double* dst, double v) { return launch("set_scalar", k_set_scalar, dim3(1), dim3(1), 0, dst, v); }
+
+  int rhs_kernel(int in_set, int out_set, int mode, int use_stage_dt, double dt) {
+    dim3 grid((g.n[0] + 127) / 128, g.n[1], g.n[2]);
+    return launch(mode ? "rhs_update" : "rhs", k_rhs<T>, grid, dim3(128), 0, (const Ctx*)dctx, g, (const T*)P, in_set,
+                  out_set, (int)kSetUs, mode, dU[0], dU[1], dU[2], rc, use_stage_dt, dt);
+  }
+
+  // ----------------------------------------------------------------- HSMAC
+  static Box bbox(const Box& a, const Box& b) {
+    Box r;
+    for (int q = 0; q < 3; q++) { r.lo[q] = std::min(a.lo[q], b.lo[q]); r.hi[q] = std::max(a.hi[q], b.hi[q]); }
+    return r;
+  }
+  static constexpr int TX = 32, TY = 8;
+  // Launch geometry of a fused sweep whose outputs cover `out`.
+  struct FusedGeom { Box gb; unsigned int gx, gy, gz; int zchunk; };
+  FusedGeom fused_geom(Box out) const {
+    FusedGeom f;
+    f.gb = bbox(out, cube(g, 1, 0));
+    const int nzc = f.gb.len(2);
+    f.gx = (f.gb.len(0) + TX - 1) / TX;
+    f.gy = (f.gb.len(1) + TY - 1) / TY;
+    // enough CTAs to fill the 148 SMs several times over: chunk z
+    int zchunk = nzc;
+    const int64_t cols = (int64_t)f.gx * f.gy;
+    while (cols * ((nzc + zchunk - 1) / zchunk) < 148 * 8 && zchunk > 16) zchunk = (zchunk + 1) / 2;
+    f.zchunk = zchunk;
+    f.gz = (nzc + zchunk - 1) / zchunk;
+    return f;
+  }
+  int fused(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks = nullptr) {
+    const FusedGeom f = fused_geom(out);
+    const int64_t nb = (int64_t)f.gx * f.gy * f.gz;
+    if (nb > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
+    if (nblocks) *nblocks = (int)nb;
+    return launch("hsmac_fused", k_hsmac_fused<T, TX, TY>, dim3(f.gx, f.gy, f.gz), dim3(TX * TY), 0, dctx, g, set, P, D,
+                  out, f.gb, fill_r, f.zchunk, hc, part, finalize, group_end, 1);
+  }
+  // in-place colour phases over a box (both colours), partial sums appended
+  int phases(int set, Box b, double* part, int* used) {
+    if (b.lo[0] > b.hi[0] || b.lo[1] > b.hi[1] || b.lo[2] > b.hi[2]) return LCS_OK;
+    if (cfg.coloring == LCS_COLORING_RED_BLACK_BLOCK) {
+      const int bs = cfg.coloring_block;
+      const int64_t nb = (int64_t)((b.len(0) + bs - 1) / bs) * ((b.len(1) + bs - 1) / bs) * ((b.len(2) + bs - 1) / bs);
+      const unsigned int gbk = blocks_for(nb, 128, 4096);
+      for (int color = 0; color <= 1; color++) {
+        LCS_TRY(launch("hsmac_block", k_hsmac_block<T>, dim3(gbk), dim3(128), 0, dctx, g, set, P, b, color, bs, hc,
+                       part + *used));
+        *used += gbk;
+      }
+      return LCS_OK;
+    }
+    const int64_t total = (int64_t)((b.len(0) + 1) / 2) * b.len(1) * b.len(2);
+    const unsigned int gbk = blocks_for(total, 256, 4096);
+    for (int color = 0; color <= 1; color++) {
+      LCS_TRY(launch("hsmac_phase", k_hsmac_phase<T>, dim3(gbk), dim3(256), 0, dctx, g, set, P, b, color, hc,
+                     part + *used));
+      *used += gbk;
+    }
+    return LCS_OK;
+  }
+  static void faces_of(Box d, Box c, Box out[6]) {  // Topologies.faces (halo.jl:349-366)
+    for (int f = 0; f < 6; f++) out[f] = d;
+    out[0].hi[2] = c.lo[2] - 1;
+    out[1].lo[2] = c.hi[2] + 1;
+    out[2].hi[1] = c.lo[1] - 1; out[2].lo[2] = c.lo[2]; out[2].hi[2] = c.hi[2];
+    out[3].lo[1] = c.hi[1] + 1; out[3].lo[2] = c.lo[2]; out[3].hi[2] = c.hi[2];
+    out[4].hi[0] = c.lo[0] - 1; out[4].lo[1] = c.lo[1]; out[4].hi[1] = c.hi[1]; out[4].lo[2] = c.lo[2]; out[4].hi[2] = c.hi[2];
+    out[5].lo[0] = c.hi[0] + 1; out[5].lo[1] = c.lo[1]; out[5].hi[1] = c.hi[1]; out[5].lo[2] = c.lo[2]; out[5].hi[2] = c.hi[2];
+  }
+  int finalize_sweep(int n, int group_end) {
+    return launch("hsmac_finalize", k_hsmac_finalize, dim3(1), dim3(256), 0, dctx, (const double*)partials, n, hc,
+                  group_end);
+  }
+  // one sweep of the phased kind: [fill +] core, then the 6 faces of dom
+  int sweep_overlap(int set, Box dom, int fill_r, int group_end) {
+    const Box core = cube(g, 2, 0);
+    int used = 0;
+    if (cfg.coloring == LCS_COLORING_RED_BLACK_BLOCK) {
+      LCS_TRY(fill(set, false, fill_r, 1));
+      LCS_TRY(phases(set, core, partials, &used));
+    } else {
+      // the fused core sweep writes every position the face phases read
+      Box out = dom;
+      for (int q = 0; q < 3; q++) { out.lo[q] -= 1; out.hi[q] = std::min(out.hi[q], g.n[q] + g.h); }
+      for (int q = 0; q < 3; q++) out.lo[q] = std::max(out.lo[q], 1 - g.h);
+      LCS_TRY(fused(set, core, out, fill_r, partials, 0, 0, &used));
+    }
+    Box f[6];
+    faces_of(dom, core, f);
+    for (int q = 0; q < 6; q++) LCS_TRY(phases(set, f[q], partials, &used));
+    return finalize_sweep(used, group_end);
+  }
+  // one plain sweep over the box D; `out` = positions the next consumer reads
+  int sweep_plain(int set, Box D, Box out, int fill_r, int group_end) {
+    if (cfg.coloring == LCS_COLORING_RED_BLACK_BLOCK) {
+      if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
+      int used = 0;
+      LCS_TRY(phases(set, D, partials, &used));
+      return finalize_sweep(used, group_end);
+    }
+    return fused(set, D, out, fill_r, partials, 1, group_end);
+  }
+  // One iteration of the reference's `while itr < itrmax` loop.
+  int couple_group(int set) {
+    const int n0 = g.n[0], h = g.h;
+    (void)n0;
+    const Box full = cube(g, 1 - h, h);
+    if (cfg.time_blocking) {  // _couple_time_blocking! (hsmac.jl:131-201)
+      const Box d1 = cube(g, -1, 3), d2 = cube(g, 0, 2), d3 = cube(g, 1, 1);
+      const Box o1 = cube(g, -1, 2), o2 = cube(g, 0, 1), o3 = cube(g, 1, 0);
+      if (cfg.overlap) {
+        LCS_TRY(sweep_overlap(set, d1, h, 0));
+      } else {
+        LCS_TRY(sweep_plain(set, d1, o1, h, 0));
+      }
+      (void)full;
+      LCS_TRY(sweep_plain(set, d2, o2, 0, 0));
+      LCS_TRY(sweep_plain(set, d3, o3, 0, 1));
+    } else {  // _couple_naive! (hsmac.jl:77-129)
+      const Box d = cube(g, 1, 1);
+      if (cfg.overlap) {
+        LCS_TRY(sweep_overlap(set, d, 1, 1));
+      } else {
+        LCS_TRY(sweep_plain(set, d, cube(g, 1, 0), 1, 1));
+      }
+    }
+    return LCS_OK;
+  }
+  int sweeps_per_group() const { return cfg.time_blocking ? 3 : 1; }
+
+  int read_ctx() {
+    LCS_TRY(copy(hctx, dctx, sizeof(Ctx), cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+
+  // Host-driven couple loop: groups are enqueued while no exit is possible
+  // (itr < itrmin), then the loop state is read back after each group.
+  int couple_direct(int stage) {
+    const int set = stage == 1 ? kSetUs2 : kSetUs;  // Us_couple (couple.jl:1-2)
+    LCS_TRY(launch("couple_reset", k_couple_reset, dim3(1), dim3(1), 0, dctx, cfg.itrmax));
+    int itr = 0;
+    const int spg = sweeps_per_group();
+    while (itr < cfg.itrmax) {
+      LCS_TRY(couple_group(set));
+      const int last_itr_in_group = itr + spg - 1;
+      if (last_itr_in_group >= cfg.itrmin) {
+        LCS_TRY(read_ctx());
+        if (hctx->nonfinite) return fail(LCS_ENONFINITE, "HSMAC residual is not finite");
+        if (hctx->cs.done) break;
+        itr = hctx->cs.itr;
+      } else {
+        itr += spg;
+      }
+    }
+    return launch("couple_log", k_couple_log, dim3(1), dim3(1), 0, dctx, stage);
+  }
+
+  // ---------------------------------------------------------------- stages
+  int forcing_stage() {
+    const int64_t ni = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const unsigned int nb = blocks_for(ni, 256, 148 * 8);
+    if (cfg.forcing == LCS_FORCING_LINEAR_POWER) {
+      LCS_TRY(fill(kSetUs, false, g.h, 1));
+      LCS_TRY(launch("lf_sums", k_lf_sums<T>, dim3(nb), dim3(256), 0, (const Ctx*)dctx, g, partials));
+      LCS_TRY(launch("lf_coef", k_lf_coef, dim3(1), dim3(256), 0, dctx, (const double*)partials, (int)nb, (double)ni,
+                     cfg.power));
+      LCS_TRY(launch("lf_apply", k_lf_apply<T>, dim3(nb), dim3(256), 0, dctx, g, partials));
+      return launch("power_mean", k_power_finalize, dim3(1), dim3(256), 0, dctx, (const double*)partials, (int)nb,
+                    (double)ni, (double)NAN);
+    }
+    if (cfg.forcing == LCS_FORCING_RC_ENERGY) {
+      const int cs = cfg.coarse_size, km = cfg.kmax;
+      const int nm = (km + 1) * (2 * km + 1) * (2 * km + 1);
+      LCS_TRY(launch("rcf_boxmean", k_rcf_boxmean<T>, dim3((3 * cs * cs * cs + 127) / 128), dim3(128), 0,
+                     (const Ctx*)dctx, g, cs, rcf_coarse));
+      LCS_TRY(launch("rcf_dft", k_rcf_dft, dim3(3 * nm), dim3(256), 0, (const double*)rcf_coarse, cs, km,
+                     (const double*)rcf_tw, rcf_hat));
+      const double norm = (double)(2 * (cs / 2 + 1) - 2) * cs * cs;
+      LCS_TRY(launch("rcf_spectrum", k_rcf_spectrum, dim3(1), dim3(32), 0, (const double*)rcf_hat, cfg.kmin, km, norm,
+                     (const double*)rcf_en0, rcf_Ac));
+      LCS_TRY(launch("rcf_apply", k_rcf_apply<T>, dim3(nb), dim3(256), 0, dctx, g, (const double*)rcf_Ac,
+                     (const double2*)ph[0], (const double2*)ph[1], (const double2*)ph[2], modes, km, partials));
+      return launch("power_mean", k_power_finalize, dim3(1), dim3(256), 0, dctx, (const double*)partials, (int)nb,
+                    (double)ni, cfg.energy);
+    }
+    return LCS_OK;
+  }
+
+  int particles_stage(int stage, int modes_mask, int use_stage_dt, double dt, int only = -1) {
+    if (cfg.mode != LCS_MODE_FLOW_PARTICLE) return LCS_OK;
+    for (int s = 0; s < cfg.n_species; s++) {
+      if (only >= 0 && s != only) continue;
+      if (sp[s].n == 0) continue;
+      LCS_TRY(launch("particles", k_particles<T>, dim3((unsigned)((sp[s].n + 255) / 256)), dim3(256), 0,
+                     (const Ctx*)dctx, g, sp[s], pc, stage, modes_mask, use_stage_dt, dt));
+    }
+    return LCS_OK;
+  }
+
+  int timestep_kernels(int flow_only, double* dout) {
+    LCS_TRY(fill(kSetUs, false, g.h, 0));  // FaceHalo(grid) (flows/timestep.jl:33)
+    const int64_t ni = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const unsigned int nb = blocks_for(ni, 256, 148 * 8);
+    LCS_TRY(launch("cfl_max", k_cfl_max<T>, dim3(nb), dim3(256), 0, (const Ctx*)dctx, g, partials));
+    return launch("cfl_finalize", k_cfl_finalize, dim3(1), dim3(256), 0, dctx, (const double*)partials, (int)nb, dc,
+                  flow_only, dout);
+  }
+
+  // evolve! body with state.dt already in ctx->dt
+  int evolve_kernels(bool direct_couple) {
+    LCS_TRY(launch("step_begin", k_step_begin, dim3(1), dim3(1), 0, dctx));
+    for (int stage = 1; stage <= 2; stage++) {
+      const int set = stage == 1 ? kSetUs : kSetUs2;
+      LCS_TRY(set_stage_dt(stage));
+      LCS_TRY(fill(set, true, g.h, 1));                 // synchalo!(FullHalo(grid), (Us.., P))
+      LCS_TRY(particles_stage(stage, 7, 1, 0.0));       // boundary!, motion!, update!
+      LCS_TRY(rhs_kernel(set, stage == 1 ? kSetUs2 : kSetUs, 1, 1, 0.0));  // rhs! + update!
+      if (stage == 2) LCS_TRY(forcing_stage());
+      if (direct_couple) LCS_TRY(couple_direct(stage));
+      else LCS_TRY(couple_graph_nodes(stage));
+    }
+    return LCS_OK;
+  }
+
+  // ------------------------------------------------------------ graph mode
+  // Appends a device-side loop for one couple to the stream being captured:
+  // reset; WHILE(cont) { group }; log.
+  int couple_graph_nodes(int stage) {
+    const int set = stage == 1 ? kSetUs2 : kSetUs;
+    LCS_TRY(launch("couple_reset", k_couple_reset, dim3(1), dim3(1), 0, dctx, cfg.itrmax));
+    cudaStreamCaptureStatus st;
+    cudaGraph_t graph;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    LCS_CUDA(cudaStreamGetCaptureInfo(stream, &st, nullptr, &graph, &deps, &ndeps));
+    if (st != cudaStreamCaptureStatusActive) return fail(LCS_ESTATE, "couple_graph_nodes outside a capture");
+    cudaGraphConditionalHandle handle;
+    LCS_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, cfg.itrmax > 0 ? 1u : 0u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    LCS_CUDA(cudaGraphAddNode(&node, graph, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    // capture the loop body on a side stream into the body graph
+    cudaStream_t main = stream;
+    cudaStream_t side;
+    LCS_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    LCS_CUDA(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    stream = side;
+    int rc2 = couple_group(set);
+    if (rc2 == LCS_OK)
+      rc2 = launch("couple_continue", k_couple_continue, dim3(1), dim3(1), 0, (const Ctx*)dctx, handle);
+    stream = main;
+    cudaGraph_t body_out;
+    cudaError_t e = cudaStreamEndCapture(side, &body_out);
+    cudaStreamDestroy(side);
+    if (rc2 != LCS_OK) return rc2;
+    if (e != cudaSuccess) return fail(LCS_ECUDA, "capture of the couple loop: %s", cudaGetErrorString(e));
+    LCS_CUDA(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+    return launch("couple_log", k_couple_log, dim3(1), dim3(1), 0, dctx, stage);
+  }
+
+  // Captures one step (with_timestep) or one evolve! into an executable graph.
+  int build_graph(bool with_timestep, cudaGraph_t* gout, cudaGraphExec_t* xout, int64_t* per_launch) {
+    if (*xout) return LCS_OK;
+    LCS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+    capturing = true;
+    const int64_t l0 = launches;
+    int rc2 = with_timestep ? timestep_kernels(0, nullptr) : LCS_OK;
+    if (rc2 == LCS_OK) rc2 = evolve_kernels(false);
+    if (rc2 == LCS_OK)
+      rc2 = launch("step_end", k_step_end, dim3(1), dim3(1), 0, dctx, with_timestep ? dlogs : (StepLog*)nullptr,
+                   (int)plan.logs_cap);
+    capturing = false;
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream, &gr);
+    if (rc2 != LCS_OK) {
+      if (gr) cudaGraphDestroy(gr);
+      return rc2;
+    }
+    if (e != cudaSuccess) return fail(LCS_ECUDA, "graph capture: %s", cudaGetErrorString(e));
+    *per_launch = launches - l0;
+    launches = l0;
+    *gout = gr;
+    LCS_CUDA(cudaGraphInstantiate(xout, gr, 0));
+    return LCS_OK;
+  }
+  int build_step_graph() { return build_graph(true, &step_graph, &step_exec, &graph_launches_per_step); }
+  int build_evolve_graph() { return build_graph(false, &evolve_graph, &evolve_exec, &graph_launches_per_evolve); }
+
+  // ------------------------------------------------------------ interface
+  int check_flow() { return uploaded_flow ? LCS_OK : fail(LCS_ESTATE, "flow fields were never uploaded"); }
+  int check_stage(int stage) { return (stage == 1 || stage == 2) ? LCS_OK : fail(LCS_EINVAL, "stage must be 1 or 2"); }
+  int check_species(int s) {
+    return (s >= 0 && s < cfg.n_species) ? LCS_OK : fail(LCS_EINVAL, "bad species index %d", s);
+  }
+
+  int upload_field(int set, int comp, T* direct, const double* host, int haloed) {
+    const int w = haloed ? g.h : 0;
+    const int64_t n = (int64_t)(g.n[0] + 2 * w) * (g.n[1] + 2 * w) * (g.n[2] + 2 * w);
+    LCS_TRY(copy(stage, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    return launch("scatter", k_scatter<T>, dim3(blocks_for(n, 256)), dim3(256), 0, (const Ctx*)dctx, g, set, comp,
+                  direct, (const double*)stage, haloed);
+  }
+  int download_field(int set, int comp, const T* direct, double* host, int haloed) {
+    const int w = haloed ? g.h : 0;
+    const int64_t n = (int64_t)(g.n[0] + 2 * w) * (g.n[1] + 2 * w) * (g.n[2] + 2 * w);
+    LCS_TRY(launch("gather", k_gather<T>, dim3(blocks_for(n, 256)), dim3(256), 0, (const Ctx*)dctx, g, set, comp,
+                   direct, stage, haloed));
+    LCS_TRY(copy(host, stage, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+
+  int upload_flow(const double* U, const double* V, const double* W, const double* Pp) override {
+    if (!U || !V || !W || !Pp) return fail(LCS_EINVAL, "null field");
+    LCS_TRY(upload_field(kSetUs, 0, nullptr, U, 0));
+    LCS_TRY(upload_field(kSetUs, 1, nullptr, V, 0));
+    LCS_TRY(upload_field(kSetUs, 2, nullptr, W, 0));
+    LCS_TRY(upload_field(-1, 0, P, Pp, 0));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    uploaded_flow = true;
+    return LCS_OK;
+  }
+  int download_flow(double* U, double* V, double* W, double* Pp) override {
+    if (U) LCS_TRY(download_field(kSetUs, 0, nullptr, U, 0));
+    if (V) LCS_TRY(download_field(kSetUs, 1, nullptr, V, 0));
+    if (W) LCS_TRY(download_field(kSetUs, 2, nullptr, W, 0));
+    if (Pp) LCS_TRY(download_field(-1, 0, P, Pp, 0));
+    return LCS_OK;
+  }
+  int field_loc(int f, int* set, int* comp, T** direct) {
+    *direct = nullptr;
+    if (f >= LCS_FIELD_U && f <= LCS_FIELD_W2) { *set = f <= LCS_FIELD_W ? kSetUs : kSetUs2; *comp = f % 3; return LCS_OK; }
+    if (f == LCS_FIELD_P) { *set = -1; *comp = 0; *direct = P; return LCS_OK; }
+    if (f >= LCS_FIELD_DUDT && f <= LCS_FIELD_DWDT) { *set = -2; *comp = f - LCS_FIELD_DUDT; *direct = dU[*comp]; return LCS_OK; }
+    return fail(LCS_EINVAL, "bad field %d", f);
+  }
+  int field_set(int f, const double* d, int haloed) override {
+    if (!d) return fail(LCS_EINVAL, "null data");
+    int set, comp;
+    T* direct;
+    LCS_TRY(field_loc(f, &set, &comp, &direct));
+    if (set == -2) {
+      const int64_t n = (int64_t)g.n[0] * g.n[1] * g.n[2];
+      LCS_TRY(copy(stage, d, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+      LCS_TRY(launch("convert", k_convert_in<T>, dim3(blocks_for(n, 256)), dim3(256), 0, direct, (const double*)stage, n));
+    } else {
+      LCS_TRY(upload_field(set, comp, direct, d, haloed));
+    }
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    if (f <= LCS_FIELD_P) uploaded_flow = true;
+    return LCS_OK;
+  }
+  int field_get(int f, double* d, int haloed) override {
+    if (!d) return fail(LCS_EINVAL, "null data");
+    int set, comp;
+    T* direct;
+    LCS_TRY(field_loc(f, &set, &comp, &direct));
+    if (set == -2) {
+      const int64_t n = (int64_t)g.n[0] * g.n[1] * g.n[2];
+      LCS_TRY(launch("convert", k_convert_out<T>, dim3(blocks_for(n, 256)), dim3(256), 0, stage, (const T*)direct, n));
+      LCS_TRY(copy(d, stage, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+      LCS_CUDA(cudaStreamSynchronize(stream));
+      return LCS_OK;
+    }
+    return download_field(set, comp, direct, d, haloed);
+  }
+
+  int refresh_particle_dt() {
+    // Particles.timestep: min over species of min(0.5 taup(max diam), dtmax)
+    double m = INFINITY;
+    for (int s = 0; s < cfg.n_species; s++) {
+      double dmax = 0.0;
+      if (sp[s].n > 0) {
+        LCS_TRY(launch("max_diam", k_max_reduce, dim3(1), dim3(256), 0, (const double*)sp[s].p[LCS_PROP_DIAM], sp[s].n,
+                       stage));
+        LCS_TRY(copy(&hctx->scal[7], stage, sizeof(double), cudaMemcpyDeviceToHost));
+        LCS_CUDA(cudaStreamSynchronize(stream));
+        dmax = hctx->scal[7];
+      }
+      const double Re = cfg.U0 * cfg.L0 / cfg.NU;
+      const double taup = 1.0 / 18.0 * cfg.species[s].density_ratio * Re * (dmax * dmax);
+      m = std::fmin(m, std::fmin(0.5 * taup, cfg.dtmax));
+    }
+    if (cfg.n_species == 0) m = cfg.dtmax;
+    return set_scalar(&dctx->dt_particles, m);
+  }
+
+  int upload_particles(int s, int64_t n, const int64_t* ids, const double* diam, const double* x, const double* y,
+                       const double* z, const double* u, const double* v, const double* w) override {
+    LCS_TRY(check_species(s));
+    if (n != sp[s].n) return fail(LCS_EINVAL, "species %d holds %lld particles, got %lld", s, (long long)sp[s].n, (long long)n);
+    const double* src[7] = {diam, x, y, z, u, v, w};
+    const int dst[7] = {LCS_PROP_DIAM, LCS_PROP_X, LCS_PROP_Y, LCS_PROP_Z, LCS_PROP_U, LCS_PROP_V, LCS_PROP_W};
+    for (int q = 0; q < 7; q++)
+      if (src[q]) LCS_TRY(copy(sp[s].p[dst[q]], src[q], (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    if (ids) LCS_TRY(copy((int64_t*)(sp[s].p[0] + 16 * n), ids, (size_t)n * 8, cudaMemcpyHostToDevice));
+    LCS_TRY(refresh_particle_dt());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int download_particles(int s, int64_t* ids, double* diam, double* x, double* y, double* z, double* u, double* v,
+                         double* w) override {
+    LCS_TRY(check_species(s));
+    double* dst[7] = {diam, x, y, z, u, v, w};
+    const int src[7] = {LCS_PROP_DIAM, LCS_PROP_X, LCS_PROP_Y, LCS_PROP_Z, LCS_PROP_U, LCS_PROP_V, LCS_PROP_W};
+    for (int q = 0; q < 7; q++)
+      if (dst[q]) LCS_TRY(copy(dst[q], sp[s].p[src[q]], (size_t)sp[s].n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (ids) LCS_TRY(copy(ids, (int64_t*)(sp[s].p[0] + 16 * sp[s].n), (size_t)sp[s].n * 8, cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int prop_set(int s, int prop, const double* d) override {
+    LCS_TRY(check_species(s));
+    if (prop < 0 || prop >= LCS_NPROP || !d) return fail(LCS_EINVAL, "bad property");
+    LCS_TRY(copy(sp[s].p[prop], d, (size_t)sp[s].n * sizeof(double), cudaMemcpyHostToDevice));
+    if (prop == LCS_PROP_DIAM) LCS_TRY(refresh_particle_dt());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int prop_get(int s, int prop, double* d) override {
+    LCS_TRY(check_species(s));
+    if (prop < 0 || prop >= LCS_NPROP || !d) return fail(LCS_EINVAL, "bad property");
+    LCS_TRY(copy(d, sp[s].p[prop], (size_t)sp[s].n * sizeof(double), cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int set_state(int64_t step, double t) override {
+    LCS_TRY(set_scalar(&dctx->t, t));
+    LCS_TRY(copy(&dctx->step, &step, sizeof(long long), cudaMemcpyHostToDevice));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int get_state(int64_t* step, double* t) override {
+    LCS_TRY(read_ctx());
+    if (step) *step = hctx->step;
+    if (t) *t = hctx->t;
+    return LCS_OK;
+  }
+
+  int timestep(double* dt) override {
+    LCS_TRY(check_flow());
+    LCS_TRY(timestep_kernels(0, nullptr));
+    LCS_TRY(collect_profile());
+    LCS_TRY(read_ctx());
+    if (hctx->nonfinite) return fail(LCS_ENONFINITE, "dt is not finite/positive");
+    if (dt) *dt = hctx->dt;
+    return LCS_OK;
+  }
+  void fill_log(const StepLog& s, lcs_log* log) {
+    log->couple1.itr = s.itr1; log->couple1.sweeps = s.sweeps1; log->couple1.div = s.div1;
+    log->couple2.itr = s.itr2; log->couple2.sweeps = s.sweeps2; log->couple2.div = s.div2;
+    log->forcing_p = s.p; log->forcing_e10 = s.e10; log->dt = s.dt; log->t = s.t; log->step = s.step;
+  }
+  int evolve(double dt, lcs_log* log) override {
+    LCS_TRY(check_flow());
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(LCS_EINVAL, "dt must be finite and positive");
+    LCS_TRY(set_scalar(&dctx->dt, dt));
+    if (cfg.use_graphs && !prof) {
+      LCS_TRY(build_evolve_graph());
+      LCS_CUDA(cudaGraphLaunch(evolve_exec, stream));
+      launches += graph_launches_per_evolve;
+    } else {
+      LCS_TRY(evolve_kernels(true));
+      LCS_TRY(launch("step_end", k_step_end, dim3(1), dim3(1), 0, dctx, (StepLog*)nullptr, 1));
+    }
+    LCS_TRY(collect_profile());
+    LCS_TRY(read_ctx());
+    if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt");
+    if (log) fill_log(hctx->cur, log);
+    return LCS_OK;
+  }
+  int step(int nsteps, lcs_log* logs) override { return step_impl(nsteps, logs, nullptr); }
+  int step_timed(int nsteps, lcs_log* logs, double* ms) override { return step_impl(nsteps, logs, ms); }
+  int transfer_stats(int64_t* h2d, int64_t* d2h) override {
+    if (h2d) *h2d = h2d_bytes;
+    if (d2h) *d2h = d2h_bytes;
+    return LCS_OK;
+  }
+  int step_impl(int nsteps, lcs_log* logs, double* ms) {
+    LCS_TRY(check_flow());
+    if (nsteps < 0) return fail(LCS_EINVAL, "nsteps < 0");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) {
+      LCS_CUDA(cudaEventCreate(&e0));
+      LCS_CUDA(cudaEventCreate(&e1));
+    }
+    int rc2 = step_body(nsteps, logs, e0, e1);
+    if (ms && rc2 == LCS_OK) {
+      float f = 0.f;
+      cudaEventElapsedTime(&f, e0, e1);
+      *ms = f;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    return rc2;
+  }
+  // Records e0 before the first step and e1 after the last one (if given).
+  int step_body(int nsteps, lcs_log* logs, cudaEvent_t e0, cudaEvent_t e1) {
+    const bool graphs = cfg.use_graphs && !prof;
+    if (graphs) LCS_TRY(build_step_graph());
+    if (e0) LCS_CUDA(cudaEventRecord(e0, stream));
+    if (!graphs) {
+      for (int q = 0; q < nsteps; q++) {
+        LCS_TRY(timestep_kernels(0, nullptr));
+        LCS_TRY(evolve_kernels(true));
+        LCS_TRY(launch("step_end", k_step_end, dim3(1), dim3(1), 0, dctx, (StepLog*)nullptr, 1));
+        if (e1 && q == nsteps - 1) LCS_CUDA(cudaEventRecord(e1, stream));
+        LCS_TRY(collect_profile());
+        LCS_TRY(read_ctx());
+        if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt at step %lld", (long long)hctx->step);
+        if (logs) fill_log(hctx->cur, &logs[q]);
+      }
+      if (e1 && nsteps == 0) LCS_CUDA(cudaEventRecord(e1, stream));
+      return LCS_OK;
+    }
+    int done = 0;
+    if (nsteps == 0 && e1) LCS_CUDA(cudaEventRecord(e1, stream));
+    while (done < nsteps) {
+      const int chunk = std::min<int>(nsteps - done, (int)plan.logs_cap);
+      for (int q = 0; q < chunk; q++) {
+        LCS_CUDA(cudaGraphLaunch(step_exec, stream));
+        launches += graph_launches_per_step;
+      }
+      if (e1 && done + chunk == nsteps) LCS_CUDA(cudaEventRecord(e1, stream));
+      LCS_TRY(read_ctx());
+      if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt near step %lld", (long long)hctx->step);
+      if (logs) {
+        std::vector<StepLog> hl(chunk);
+        for (int q = 0; q < chunk; q++) {
+          const long long st = hctx->step - chunk + q + 1;
+          LCS_TRY(copy(&hl[q], dlogs + (st - 1) % plan.logs_cap, sizeof(StepLog), cudaMemcpyDeviceToHost));
+        }
+        LCS_CUDA(cudaStreamSynchronize(stream));
+        for (int q = 0; q < chunk; q++) fill_log(hl[q], &logs[done + q]);
+      }
+      done += chunk;
+    }
+    return LCS_OK;
+  }
+
+  int synchalo(int mask, int r, int full) override {
+    if (r < 0 || r > g.h) return fail(LCS_EINVAL, "halo width out of range");
+    const bool us = mask & 7, us2 = (mask >> 3) & 7, withP = (mask >> LCS_FIELD_P) & 1;
+    if (us) LCS_TRY(fill(kSetUs, false, r, full));
+    if (us2) LCS_TRY(fill(kSetUs2, false, r, full));
+    if (withP) LCS_TRY(fill(-1, true, r, full));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int rhs(int stage) override {
+    LCS_TRY(check_stage(stage));
+    LCS_TRY(rhs_kernel(stage == 1 ? kSetUs : kSetUs2, 0, 0, 0, 0.0));
+    LCS_TRY(collect_profile());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int update(int stage, double dtrk) override {
+    LCS_TRY(check_stage(stage));
+    dim3 grid((g.n[0] + 127) / 128, g.n[1], g.n[2]);
+    LCS_TRY(launch("update", k_update<T>, grid, dim3(128), 0, (const Ctx*)dctx, g, stage == 1 ? (int)kSetUs2 : (int)kSetUs,
+                   (int)kSetUs, (const T*)dU[0], (const T*)dU[1], (const T*)dU[2], dtrk));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int rhs_update(int stage, double dtrk) override {
+    LCS_TRY(check_stage(stage));
+    LCS_TRY(rhs_kernel(stage == 1 ? kSetUs : kSetUs2, stage == 1 ? kSetUs2 : kSetUs, 1, 0, dtrk));
+    LCS_TRY(collect_profile());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int couple(int stage, double dtrk, lcs_couple_log* log) override {
+    LCS_TRY(check_stage(stage));
+    LCS_TRY(set_scalar(&dctx->scal[0], dtrk));
+    LCS_TRY(couple_direct(stage));
+    LCS_TRY(collect_profile());
+    LCS_TRY(read_ctx());
+    if (hctx->nonfinite) return fail(LCS_ENONFINITE, "HSMAC residual is not finite");
+    if (log) {
+      log->itr = hctx->cs.itr;
+      log->sweeps = hctx->cs.sweeps;
+      log->div = hctx->cs.div;
+    }
+    return LCS_OK;
+  }
+  int forcing(double dtrk, double* p, double* e10) override {
+    LCS_TRY(set_scalar(&dctx->scal[0], dtrk));
+    LCS_TRY(launch("step_begin", k_step_begin, dim3(1), dim3(1), 0, dctx));
+    LCS_TRY(forcing_stage());
+    LCS_TRY(collect_profile());
+    LCS_TRY(read_ctx());
+    if (p) *p = hctx->cur.p;
+    if (e10) *e10 = hctx->cur.e10;
+    return LCS_OK;
+  }
+  int flow_timestep(double* dt) override {
+    LCS_TRY(timestep_kernels(1, stage));
+    LCS_TRY(copy(&hctx->scal[7], stage, sizeof(double), cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    if (dt) *dt = hctx->scal[7];
+    return LCS_OK;
+  }
+  int particles_timestep(double* dt) override {
+    LCS_TRY(read_ctx());
+    if (dt) *dt = (cfg.mode == LCS_MODE_FLOW_PARTICLE && cfg.n_species > 0) ? hctx->dt_particles : cfg.dtmax;
+    return LCS_OK;
+  }
+  int particles_boundary(int s, int stage) override {
+    LCS_TRY(check_species(s));
+    LCS_TRY(check_stage(stage));
+    LCS_TRY(particles_stage(stage, 1, 0, 0.0, s));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int particles_motion(int s, int stage) override {
+    LCS_TRY(check_species(s));
+    LCS_TRY(check_stage(stage));
+    LCS_TRY(particles_stage(stage, 2, 0, 0.0, s));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int particles_update(int s, int stage, double dtrk) override {
+    LCS_TRY(check_species(s));
+    LCS_TRY(check_stage(stage));
+    LCS_TRY(particles_stage(stage, 4, 0, dtrk, s));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int init_particle_velocity(int s) override {
+    LCS_TRY(check_species(s));
+    LCS_TRY(fill(kSetUs, false, g.h, 1));
+    if (sp[s].n > 0)
+      LCS_TRY(launch("particles_init_velocity", k_particles_init_velocity<T>, dim3((unsigned)((sp[s].n + 255) / 256)),
+                     dim3(256), 0, (const Ctx*)dctx, g, sp[s], pc));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+
+  int profile_enable(int on) override {
+    prof = on != 0;
+    return LCS_OK;
+  }
+  int profile_reset() override {
+    LCS_TRY(collect_profile());
+    totals.clear();
+    launches = 0;
+    return LCS_OK;
+  }
+  int profile_count(int* n) override {
+    LCS_TRY(collect_profile());
+    *n = (int)totals.size();
+    return LCS_OK;
+  }
+  int profile_entry(int i, char* name, int cap, double* ms, int64_t* n) override {
+    if (i < 0 || i >= (int)totals.size()) return fail(LCS_EINVAL, "profile index out of range");
+    if (name && cap > 0) {
+      strncpy(name, totals[i].label.c_str(), cap - 1);
+      name[cap - 1] = 0;
+    }
+    if (ms) *ms = totals[i].ms;
+    if (n) *n = totals[i].n;
+    return LCS_OK;
+  }
+  int launch_count(int64_t* n) override {
+    *n = launches;
+    return LCS_OK;
+  }
+  int synchronize() override {
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+};
+
+}  // namespace lcs

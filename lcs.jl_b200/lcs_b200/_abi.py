@@ -1,0 +1,192 @@
+"""ctypes mirror of include/lcs_b200.h and the loader of liblcs_b200.so.
+
+The structures below are byte-for-byte the C structs of the header; the test
+``tests/test_abi.py`` checks their sizes and field offsets against a C
+compilation of the header.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+ABI_VERSION = 1
+MAX_SPECIES = 16
+
+OK = 0
+EINVAL = -1
+ENOMEM = -2
+ECUDA = -3
+ETIMEDOUT = -4
+ENONFINITE = -5
+ESTATE = -6
+
+ERROR_NAMES = {
+    EINVAL: "EINVAL",
+    ENOMEM: "ENOMEM",
+    ECUDA: "ECUDA",
+    ETIMEDOUT: "ETIMEDOUT",
+    ENONFINITE: "ENONFINITE",
+    ESTATE: "ESTATE",
+}
+
+MODE_FLOW, MODE_FLOW_PARTICLE = 0, 1
+COLORING_NO, COLORING_RED_BLACK, COLORING_RED_BLACK_FAST, COLORING_RED_BLACK_BLOCK = 0, 1, 2, 3
+FORCING_NO, FORCING_LINEAR_POWER, FORCING_RC_ENERGY = 0, 1, 2
+DRAG_LINEAR, DRAG_NONLINEAR = 0, 1
+PRECISION_FP64, PRECISION_FP32_MIXED = 0, 1
+
+FIELD_U, FIELD_V, FIELD_W, FIELD_U2, FIELD_V2, FIELD_W2, FIELD_P, FIELD_DUDT, FIELD_DVDT, FIELD_DWDT = range(10)
+FIELD_NAMES = ["U", "V", "W", "U2", "V2", "W2", "P", "dUdt", "dVdt", "dWdt"]
+
+(PROP_X, PROP_Y, PROP_Z, PROP_X2, PROP_Y2, PROP_Z2, PROP_U, PROP_V, PROP_W, PROP_U2, PROP_V2, PROP_W2,
+ PROP_DUDT, PROP_DVDT, PROP_DWDT, PROP_DIAM) = range(16)
+NPROP = 16
+PROP_NAMES = ["x", "y", "z", "x2", "y2", "z2", "u", "v", "w", "u2", "v2", "w2", "dudt", "dvdt", "dwdt", "diam"]
+
+
+class Species(C.Structure):
+    _fields_ = [
+        ("nvalid", C.c_int64),
+        ("gravity", C.c_double),
+        ("density_ratio", C.c_double),
+        ("drag", C.c_int32),
+        ("_pad", C.c_int32),
+    ]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32),
+        ("mode", C.c_int32),
+        ("dims", C.c_int32 * 3),
+        ("halo_size", C.c_int32),
+        ("cfl", C.c_double),
+        ("dtmax", C.c_double),
+        ("U0", C.c_double),
+        ("L0", C.c_double),
+        ("NU", C.c_double),
+        ("time_blocking", C.c_int32),
+        ("overlap", C.c_int32),
+        ("coloring", C.c_int32),
+        ("coloring_block", C.c_int32),
+        ("omega", C.c_double),
+        ("epsp", C.c_double),
+        ("itrmin", C.c_int32),
+        ("itrmax", C.c_int32),
+        ("forcing", C.c_int32),
+        ("kmin", C.c_int32),
+        ("kmax", C.c_int32),
+        ("coarse_size", C.c_int32),
+        ("power", C.c_double),
+        ("energy", C.c_double),
+        ("n_species", C.c_int32),
+        ("precision", C.c_int32),
+        ("species", Species * MAX_SPECIES),
+        ("device", C.c_int32),
+        ("use_graphs", C.c_int32),
+    ]
+
+
+class CoupleLog(C.Structure):
+    _fields_ = [("itr", C.c_int32), ("sweeps", C.c_int32), ("div", C.c_double)]
+
+
+class Log(C.Structure):
+    _fields_ = [
+        ("couple1", CoupleLog),
+        ("couple2", CoupleLog),
+        ("forcing_p", C.c_double),
+        ("forcing_e10", C.c_double),
+        ("dt", C.c_double),
+        ("t", C.c_double),
+        ("step", C.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {
+            "couple1": {"itr": self.couple1.itr, "sweeps": self.couple1.sweeps, "div": self.couple1.div},
+            "couple2": {"itr": self.couple2.itr, "sweeps": self.couple2.sweeps, "div": self.couple2.div},
+            "forcing": {"p": self.forcing_p, "e10": self.forcing_e10},
+            "dt": self.dt,
+            "t": self.t,
+            "step": self.step,
+        }
+
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I64 = C.POINTER(C.c_int64)
+
+# name -> (restype, argtypes) for every entry point of include/lcs_b200.h
+PROTOTYPES = {
+    "lcs_create": (C.c_int, [C.POINTER(Config), C.POINTER(_P)]),
+    "lcs_destroy": (None, [_P]),
+    "lcs_last_error": (C.c_char_p, [_P]),
+    "lcs_footprint": (C.c_int, [C.POINTER(Config), _I64]),
+    "lcs_upload_flow": (C.c_int, [_P, _D, _D, _D, _D]),
+    "lcs_download_flow": (C.c_int, [_P, _D, _D, _D, _D]),
+    "lcs_field_set": (C.c_int, [_P, C.c_int32, _D, C.c_int32]),
+    "lcs_field_get": (C.c_int, [_P, C.c_int32, _D, C.c_int32]),
+    "lcs_upload_particles": (C.c_int, [_P, C.c_int32, C.c_int64, _I64, _D, _D, _D, _D, _D, _D, _D]),
+    "lcs_download_particles": (C.c_int, [_P, C.c_int32, _I64, _D, _D, _D, _D, _D, _D, _D]),
+    "lcs_prop_set": (C.c_int, [_P, C.c_int32, C.c_int32, _D]),
+    "lcs_prop_get": (C.c_int, [_P, C.c_int32, C.c_int32, _D]),
+    "lcs_set_state": (C.c_int, [_P, C.c_int64, C.c_double]),
+    "lcs_get_state": (C.c_int, [_P, _I64, _D]),
+    "lcs_timestep": (C.c_int, [_P, _D]),
+    "lcs_evolve": (C.c_int, [_P, C.c_double, C.POINTER(Log)]),
+    "lcs_step": (C.c_int, [_P, C.c_int32, C.POINTER(Log)]),
+    "lcs_step_timed": (C.c_int, [_P, C.c_int32, C.POINTER(Log), _D]),
+    "lcs_transfer_stats": (C.c_int, [_P, _I64, _I64]),
+    "lcs_synchalo": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
+    "lcs_flow_rhs": (C.c_int, [_P, C.c_int32]),
+    "lcs_flow_update": (C.c_int, [_P, C.c_int32, C.c_double]),
+    "lcs_flow_rhs_update": (C.c_int, [_P, C.c_int32, C.c_double]),
+    "lcs_flow_couple": (C.c_int, [_P, C.c_int32, C.c_double, C.POINTER(CoupleLog)]),
+    "lcs_flow_forcing": (C.c_int, [_P, C.c_double, _D, _D]),
+    "lcs_flow_timestep": (C.c_int, [_P, _D]),
+    "lcs_particles_timestep": (C.c_int, [_P, _D]),
+    "lcs_particles_boundary": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "lcs_particles_motion": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "lcs_particles_update": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_double]),
+    "lcs_init_particle_velocity": (C.c_int, [_P, C.c_int32]),
+    "lcs_profile_enable": (C.c_int, [_P, C.c_int32]),
+    "lcs_profile_reset": (C.c_int, [_P]),
+    "lcs_profile_count": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "lcs_profile_entry": (C.c_int, [_P, C.c_int32, C.c_char_p, C.c_int32, _D, _I64]),
+    "lcs_launch_count": (C.c_int, [_P, _I64]),
+    "lcs_synchronize": (C.c_int, [_P]),
+}
+
+PACKAGE_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBRARY_PATH = os.path.join(PACKAGE_DIR, "liblcs_b200.so")
+
+
+def bind(lib: C.CDLL) -> C.CDLL:
+    """Attach the prototypes of every ABI entry point to a loaded library."""
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_cuda_lib = None
+
+
+def load_library() -> C.CDLL:
+    """Load the in-tree CUDA library; raise if it was not built.
+
+    There is no CPU fallback: the time step runs on the B200 kernels or not at
+    all.
+    """
+    global _cuda_lib
+    if _cuda_lib is None:
+        if not os.path.exists(LIBRARY_PATH):
+            raise RuntimeError(
+                f"{LIBRARY_PATH} is missing: build it with `make -C lcs.jl_b200` "
+                "(or __graft_entry__.build()); the B200 backend has no CPU fallback"
+            )
+        _cuda_lib = bind(C.CDLL(LIBRARY_PATH))
+    return _cuda_lib

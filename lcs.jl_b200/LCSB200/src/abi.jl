@@ -1,0 +1,102 @@
+# ccall bindings of include/lcs_b200.h (the C ABI of liblcs_b200.so).
+const LIB = joinpath(@__DIR__, "..", "..", "liblcs_b200.so")
+const MAX_SPECIES = 16
+
+struct LcsSpecies
+    nvalid::Int64
+    gravity::Float64
+    density_ratio::Float64
+    drag::Int32
+    _pad::Int32
+end
+
+struct LcsConfig
+    abi_version::Int32
+    mode::Int32
+    dims::NTuple{3,Int32}
+    halo_size::Int32
+    cfl::Float64
+    dtmax::Float64
+    U0::Float64
+    L0::Float64
+    NU::Float64
+    time_blocking::Int32
+    overlap::Int32
+    coloring::Int32
+    coloring_block::Int32
+    omega::Float64
+    epsp::Float64
+    itrmin::Int32
+    itrmax::Int32
+    forcing::Int32
+    kmin::Int32
+    kmax::Int32
+    coarse_size::Int32
+    power::Float64
+    energy::Float64
+    n_species::Int32
+    precision::Int32
+    species::NTuple{MAX_SPECIES,LcsSpecies}
+    device::Int32
+    use_graphs::Int32
+end
+
+struct LcsCoupleLog
+    itr::Int32
+    sweeps::Int32
+    div::Float64
+end
+
+struct LcsLog
+    couple1::LcsCoupleLog
+    couple2::LcsCoupleLog
+    p::Float64
+    e10::Float64
+    dt::Float64
+    t::Float64
+    step::Int64
+end
+
+lasterror(h) = unsafe_string(ccall((:lcs_last_error, LIB), Cstring, (Ptr{Cvoid},), h))
+check(h, rc) = rc == 0 || throw(ArgumentError("lcs_b200: " * lasterror(h)))
+
+function create(cfg::LcsConfig)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(C_NULL, ccall((:lcs_create, LIB), Cint, (Ref{LcsConfig}, Ref{Ptr{Cvoid}}), cfg, r))
+    r[]
+end
+destroy(h) = ccall((:lcs_destroy, LIB), Cvoid, (Ptr{Cvoid},), h)
+
+upload_flow!(h, U, V, W, P) = check(h, ccall((:lcs_upload_flow, LIB), Cint,
+    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), h, U, V, W, P))
+download_flow!(h, U, V, W, P) = check(h, ccall((:lcs_download_flow, LIB), Cint,
+    (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), h, U, V, W, P))
+
+function upload_particles!(h, s, ids, diam, x, y, z, u, v, w)
+    n = length(x)
+    check(h, ccall((:lcs_upload_particles, LIB), Cint,
+        (Ptr{Cvoid}, Int32, Int64, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+         Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), h, s, n, ids, diam, x, y, z, u, v, w))
+end
+function download_particles!(h, s, ids, diam, x, y, z, u, v, w)
+    check(h, ccall((:lcs_download_particles, LIB), Cint,
+        (Ptr{Cvoid}, Int32, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+         Ptr{Float64}, Ptr{Float64}, Ptr{Float64}), h, s, ids, diam, x, y, z, u, v, w))
+end
+
+function timestep(h)
+    dt = Ref{Float64}()
+    check(h, ccall((:lcs_timestep, LIB), Cint, (Ptr{Cvoid}, Ref{Float64}), h, dt))
+    dt[]
+end
+function evolve!(h, dt::Float64)
+    lg = Ref{LcsLog}()
+    check(h, ccall((:lcs_evolve, LIB), Cint, (Ptr{Cvoid}, Float64, Ref{LcsLog}), h, dt, lg))
+    lg[]
+end
+function step!(h, n::Integer)
+    logs = Vector{LcsLog}(undef, n)
+    check(h, ccall((:lcs_step, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{LcsLog}), h, n, logs))
+    logs
+end
+set_state!(h, step, t) = check(h, ccall((:lcs_set_state, LIB), Cint, (Ptr{Cvoid}, Int64, Float64), h, step, t))

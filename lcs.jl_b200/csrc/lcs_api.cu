@@ -60,7 +60,12 @@ static int validate(const lcs_config* c, std::string* why) {
   }
   if (c->n_species < 0 || c->n_species > LCS_MAX_SPECIES) { *why = "n_species out of range"; return LCS_EINVAL; }
   for (int s = 0; s < c->n_species; s++) {
-    if (c->species[s].nvalid < 0) { *why = "negative particle count"; return LCS_EINVAL; }
+    // Particles.timestep reduces `maximum` over the species' diameters, which
+    // throws for an empty species in the reference (src/particles/timestep.jl:22)
+    if (c->mode == LCS_MODE_FLOW_PARTICLE && c->species[s].nvalid < 1) {
+      *why = "every particle species needs at least one particle";
+      return LCS_EINVAL;
+    }
     if (c->species[s].drag != LCS_DRAG_LINEAR && c->species[s].drag != LCS_DRAG_NONLINEAR) { *why = "bad drag kind"; return LCS_EINVAL; }
     if (!(c->species[s].density_ratio > 0)) { *why = "density_ratio must be positive"; return LCS_EINVAL; }
   }

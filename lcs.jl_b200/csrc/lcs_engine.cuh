@@ -277,7 +277,7 @@ class Engine : public EngineBase {
       host_kset(K, ks);
     }
     modes.kofs[modes.nshell] = (int)ks.size();
-    if (ks.size() > 128) return fail(LCS_EINVAL, "rc-energy kset too large (%zu modes)", ks.size());
+    if (ks.size() > 256) return fail(LCS_EINVAL, "rc-energy kset too large (%zu modes)", ks.size());
     modes.n = (int)ks.size();
     for (size_t q = 0; q < ks.size(); q++)
       for (int a = 0; a < 3; a++) modes.k[q][a] = (signed char)ks[q][a];
@@ -505,7 +505,11 @@ class Engine : public EngineBase {
     LCS_TRY(launch("couple_reset", k_couple_reset, dim3(1), dim3(1), 0, dctx, cfg.itrmax));
     int itr = 0;
     const int spg = sweeps_per_group();
-    while (itr < cfg.itrmax) {
+    // the device advances itr by one per sweep until it exits; the group
+    // count is bounded so the host loop ends even if that ever failed
+    const int max_groups = cfg.itrmax / spg + 2;
+    for (int grp = 0; itr < cfg.itrmax; grp++) {
+      if (grp >= max_groups) return fail(LCS_ETIMEDOUT, "HSMAC loop did not advance");
       LCS_TRY(couple_group(set));
       const int last_itr_in_group = itr + spg - 1;
       if (last_itr_in_group >= cfg.itrmin) {

@@ -887,7 +887,7 @@ struct RcfModes {
   int n;
   int nshell;
   int kofs[9];
-  signed char k[128][3];
+  signed char k[256][3];  // kset(1..4): 9 + 31 + 49 + 105 vectors
 };
 
 template <typename T>
@@ -896,8 +896,8 @@ __global__ void __launch_bounds__(256) k_rcf_apply(Ctx* __restrict__ ctx, Grid g
                                                    const double2* __restrict__ phz, RcfModes md, int kmax,
                                                    double* __restrict__ partials) {
   __shared__ double sh[8];
-  __shared__ double2 sA[3][128];
-  __shared__ signed char sk[128][3];
+  __shared__ double2 sA[3][256];
+  __shared__ signed char sk[256][3];
   const int KX = kmax + 1, KY = 2 * kmax + 1, nm = KX * KY * KY;
   for (int q = threadIdx.x; q < md.n; q += blockDim.x) {
     const int kx = md.k[q][0], ky = md.k[q][1], kz = md.k[q][2];

@@ -658,8 +658,8 @@ static double forcing_rcf(lcs_handle* h, double dt, double* e10_out) {
       ph[a][i].im = s;
     }
   }
-  int ks[64][3], kofs[16], nk = 0;
-  for (int K = kmin; K <= kmax; K++) { kofs[K - kmin] = nk; nk += kset(K, ks + nk, 64 - nk); }
+  int ks[256][3], kofs[16], nk = 0; /* kset(1..4) hold 9 + 31 + 49 + 105 vectors */
+  for (int K = kmin; K <= kmax; K++) { kofs[K - kmin] = nk; nk += kset(K, ks + nk, 256 - nk); }
   kofs[kmax - kmin + 1] = nk;
 #pragma omp parallel for schedule(static)
   for (int k = 1; k <= g->n[2]; k++)
@@ -853,6 +853,9 @@ int lcs_create(const lcs_config* cfg, lcs_handle** out) {
     if (cfg->dims[a] < 4 || cfg->dims[a] % 2) return fail(NULL, LCS_EINVAL, "dims must be even and >= 4");
   if (cfg->halo_size < 3) return fail(NULL, LCS_EINVAL, "halo_size must be >= 3");
   if (cfg->n_species < 0 || cfg->n_species > LCS_MAX_SPECIES) return fail(NULL, LCS_EINVAL, "bad n_species");
+  /* maximum(diams) over an empty species throws in the reference (src/particles/timestep.jl:22) */
+  for (int s = 0; cfg->mode == LCS_MODE_FLOW_PARTICLE && s < cfg->n_species; s++)
+    if (cfg->species[s].nvalid < 1) return fail(NULL, LCS_EINVAL, "every particle species needs at least one particle");
   if (cfg->coloring == LCS_COLORING_RED_BLACK_BLOCK && cfg->coloring_block < 1)
     return fail(NULL, LCS_EINVAL, "red-black-block needs size >= 1");
   if (cfg->forcing == LCS_FORCING_RC_ENERGY) {
@@ -1152,8 +1155,8 @@ int lcs_synchronize(lcs_handle* h) { return h ? LCS_OK : LCS_EINVAL; }
 /* ---- oracle-only helpers for the known-answer tests -------------------- */
 int lcs_oracle_kcount(int k0) { return kcount(k0); }
 int lcs_oracle_kset(int k0, int32_t* out, int cap) {
-  int tmp[128][3];
-  int n = kset(k0, tmp, cap < 128 ? cap : 128);
+  int tmp[256][3];
+  int n = kset(k0, tmp, cap < 256 ? cap : 256);
   for (int q = 0; q < n; q++) { out[3 * q] = tmp[q][0]; out[3 * q + 1] = tmp[q][1]; out[3 * q + 2] = tmp[q][2]; }
   return n;
 }
@@ -1178,12 +1181,12 @@ void lcs_oracle_boxmean(const double* A, int n, int h, int c, double* out) {
 /* sirdft of a cropped spectrum Ac[kz][ky][kx] (sizes 2kmax+1, 2kmax+1, kmax+1) at phases ei,ej,ek */
 double lcs_oracle_sirdft(const double* Ac_reim, int kmin, int kmax, double eir, double eii, double ejr, double eji,
                          double ekr, double eki) {
-  int ks[128][3];
+  int ks[256][3];
   const int KX = kmax + 1, KY = 2 * kmax + 1;
   cplx ei = {eir, eii}, ej = {ejr, eji}, ek = {ekr, eki};
   double tot = 0.0;
   for (int K = kmin; K <= kmax; K++) {
-    int n = kset(K, ks, 128);
+    int n = kset(K, ks, 256);
     double acc = 0.0;
     for (int q = 0; q < n; q++) {
       int kx = ks[q][0], ky = ks[q][1], kz = ks[q][2];

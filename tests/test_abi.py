@@ -87,6 +87,8 @@ def test_footprint_and_validation_without_gpu(cuda_lib_path):
     assert lib.lcs_footprint(C.byref(nocol), C.byref(b)) == _abi.EINVAL
     rcf = make_config(16, forcing=_abi.FORCING_RC_ENERGY, kmin=1, kmax=3, coarse=4)
     assert lib.lcs_footprint(C.byref(rcf), C.byref(b)) == _abi.EINVAL
+    empty = make_config(16, species=[{"n": 0}])
+    assert lib.lcs_footprint(C.byref(empty), C.byref(b)) == _abi.EINVAL
 
 
 @pytest.mark.skipif(gpu_available(), reason="checks the no-GPU refusal")

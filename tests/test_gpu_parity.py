@@ -286,12 +286,16 @@ def test_graph_step_equals_direct_calls():
     assert [x["couple2"]["itr"] for x in la] == [x["couple2"]["itr"] for x in lb]
 
 
-def test_empty_species_and_flow_mode():
-    cfg = make_config(16, forcing=F.FORCING_LINEAR_POWER, power=0.5, Re=50.0, itrmax=12,
-                      species=[{"n": 0}, {"n": 10}])
-    (g, o), (lg, lo) = evolve_pair(cfg, 2, nparts=(0, 10))
-    for a, b in zip(g.download_flow(), o.download_flow()):
-        assert rel_l2(a, b) <= 1e-12
+def test_empty_species_rejected_and_flow_mode():
+    """An empty species makes the reference's `maximum(diams)` throw; both
+    libraries refuse it at create time.  FlowMode (no particles) runs."""
+    from lcs_b200 import LCSError
+
+    bad = make_config(16, species=[{"n": 0}, {"n": 10}])
+    for cls in (Engine, OracleEngine):
+        with pytest.raises(LCSError) as ei:
+            cls(bad)
+        assert ei.value.code == F.EINVAL
     cfg = make_config(16, mode=F.MODE_FLOW, forcing=F.FORCING_NO, Re=50.0, itrmax=12)
     (g, o), _ = evolve_pair(cfg, 2, nparts=())
     for a, b in zip(g.download_flow(), o.download_flow()):

@@ -222,6 +222,25 @@ LCS_API int lcs_launch_count(lcs_handle* h, int64_t* launches);
 LCS_API int lcs_transfer_stats(lcs_handle* h, int64_t* h2d_bytes, int64_t* d2h_bytes);
 LCS_API int lcs_synchronize(lcs_handle* h);
 
+/* ---- allocation-free variant --------------------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library
+ * call cudaMalloc: code recording a CUDA stream capture, or a process whose
+ * device memory belongs to another allocator (a Julia CUDA.jl pool, a server
+ * with a fixed per-request budget).  Computes `Flows.timestep`'s dt from U, V,
+ * W device arrays the caller owns, laid out as the reference's haloed fields
+ * ((n+2h)^3 FP64, x fastest; only the interior is read) and writes it to the
+ * caller's device double *dt_out, on `stream` (a cudaStream_t, NULL for the
+ * default stream).  It allocates nothing: its scratch is a static device array
+ * of 3 * LCS_NOALLOC_MAX_PLANES doubles per GPU, held until the process exits,
+ * so dims[2] may be at most LCS_NOALLOC_MAX_PLANES (larger grids get EINVAL).
+ * The first call on a device looks the array up and should come before any
+ * stream capture.  Every call shares the array: calls that overlap on the GPU
+ * race.  Errors are reported through lcs_last_error(NULL). */
+#define LCS_NOALLOC_MAX_PLANES 4096
+LCS_API int lcs_flow_timestep_noalloc(const double* U, const double* V, const double* W, const int32_t dims[3],
+                                      int32_t halo_size, double cfl, double dtmax, double Re, double* dt_out,
+                                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,11 @@ static int set_global_error(int code, const char* msg) {
   return code;
 }
 
+namespace lcs {
+// Error text of the handle-less entry points, read by lcs_last_error(NULL).
+void set_global_error_message(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+}  // namespace lcs
+
 // Config checks shared by lcs_create and lcs_footprint (the reference's
 // constructors throw ArgumentError for the same cases).
 static int validate(const lcs_config* c, std::string* why) {

@@ -157,7 +157,11 @@ PROTOTYPES = {
     "lcs_profile_entry": (C.c_int, [_P, C.c_int32, C.c_char_p, C.c_int32, _D, _I64]),
     "lcs_launch_count": (C.c_int, [_P, _I64]),
     "lcs_synchronize": (C.c_int, [_P]),
+    "lcs_flow_timestep_noalloc": (C.c_int, [_P, _P, _P, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_double,
+                                            C.c_double, _P, _P]),
 }
+
+NOALLOC_MAX_PLANES = 4096
 
 PACKAGE_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIBRARY_PATH = os.path.join(PACKAGE_DIR, "liblcs_b200.so")

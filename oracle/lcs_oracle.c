@@ -1243,3 +1243,38 @@ double lcs_oracle_enespe(const double* hat_reim, int kmax, int k0, double norm) 
   return enespe_cropped((const cplx*)hat_reim, kmax, k0, norm);
 }
 double lcs_oracle_phase_shift(int n, int coarse_size) { return (double)(n / coarse_size) / 2.0; }
+
+/* The same dt as lcs_flow_timestep, on caller-owned (here: host) arrays in the
+ * reference's haloed layout, reading the interior with periodic wrapping. */
+int lcs_flow_timestep_noalloc(const double* U, const double* V, const double* W, const int32_t dims[3],
+                              int32_t halo, double cfl, double dtmax, double Re, double* dt_out, void* stream) {
+  (void)stream;
+  if (!U || !V || !W || !dims || !dt_out) return fail(NULL, LCS_EINVAL, "null argument");
+  if (dims[2] > LCS_NOALLOC_MAX_PLANES) return fail(NULL, LCS_EINVAL, "dims[2] exceeds LCS_NOALLOC_MAX_PLANES");
+  grid_t g;
+  for (int a = 0; a < 3; a++) { g.n[a] = dims[a]; g.s[a] = dims[a] + 2 * halo; }
+  g.h = halo;
+  double mx[3] = {0, 0, 0};
+  for (int k = 1; k <= g.n[2]; k++)
+    for (int j = 1; j <= g.n[1]; j++)
+      for (int i = 1; i <= g.n[0]; i++) {
+        const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+        double uc = interp_o4_at_half(U[IX(&g, wrap1(i - 2, nx), j, k)], U[IX(&g, wrap1(i - 1, nx), j, k)],
+                                      U[IX(&g, i, j, k)], U[IX(&g, wrap1(i + 1, nx), j, k)]);
+        double vc = interp_o4_at_half(V[IX(&g, i, wrap1(j - 2, ny), k)], V[IX(&g, i, wrap1(j - 1, ny), k)],
+                                      V[IX(&g, i, j, k)], V[IX(&g, i, wrap1(j + 1, ny), k)]);
+        double wc = interp_o4_at_half(W[IX(&g, i, j, wrap1(k - 2, nz))], W[IX(&g, i, j, wrap1(k - 1, nz))],
+                                      W[IX(&g, i, j, k)], W[IX(&g, i, j, wrap1(k + 1, nz))]);
+        mx[0] = fmax(mx[0], fabs(uc));
+        mx[1] = fmax(mx[1], fabs(vc));
+        mx[2] = fmax(mx[2], fabs(wc));
+      }
+  double dx = DOMAIN_LENGTH / g.n[0], dy = DOMAIN_LENGTH / g.n[1], dz = DOMAIN_LENGTH / g.n[2];
+  double d = dtmax;
+  d = fmin(d, cfl * dx / (mx[0] + 1e-10));
+  d = fmin(d, cfl * dy / (mx[1] + 1e-10));
+  d = fmin(d, cfl * dz / (mx[2] + 1e-10));
+  d = fmin(d, 0.5 * ((dx / 2.0) * (dx / 2.0)) / (1.0 / Re));
+  *dt_out = d;
+  return LCS_OK;
+}

@@ -85,6 +85,7 @@ struct StepLog {
 // from here, so the same launches serve direct calls and graph replays.
 struct Ctx {
   void* vel[3][3];      // [set][component] haloed velocity buffers
+  int vphys[3][3];      // [set][component] index 0..8 of the physical buffer (tensor map)
   double dt;            // state.dt
   double t;             // state.t
   long long step;       // state.step
@@ -94,6 +95,7 @@ struct Ctx {
   StepLog cur;          // log of the step in progress
   unsigned int ticket;  // last-block-done counter
   int nonfinite;        // sticky: a NaN/Inf dt or residual was seen
+  int tma_error;        // sticky: a bounded wait on a TMA copy ran out
 };
 
 // ---- stencil primitives (src/diff.jl:1-39), same evaluation order --------

@@ -17,8 +17,13 @@
 #include <vector>
 
 #include "../../include/lcs_b200.h"
+#include <cudaTypedefs.h>
+
+#include <cstdlib>
+
 #include "lcs_base.h"
 #include "lcs_kernels.cuh"
+#include "lcs_hsmac_tma.cuh"
 
 namespace lcs {
 
@@ -214,7 +219,10 @@ class Engine : public EngineBase {
     Ctx h0;
     memset(&h0, 0, sizeof h0);
     for (int s = 0; s < 3; s++)
-      for (int q = 0; q < 3; q++) h0.vel[s][q] = vel0[s][q];
+      for (int q = 0; q < 3; q++) {
+        h0.vel[s][q] = vel0[s][q];
+        h0.vphys[s][q] = 3 * s + q;
+      }
     h0.dt_particles = c.dtmax;
     h0.cur.p = NAN;
     h0.cur.e10 = NAN;
@@ -246,9 +254,64 @@ class Engine : public EngineBase {
     dc.with_particles = c.mode == LCS_MODE_FLOW_PARTICLE && c.n_species > 0;
     pc.dx = dx; pc.dy = dy; pc.dz = dz; pc.Re = Re;
     if (c.forcing == LCS_FORCING_RC_ENERGY) LCS_TRY(init_rcf());
+    // the TMA-fed sweep serves red-black-fast (the production colouring);
+    // LCS_B200_FUSED_SWEEP=plain selects the plain-load sweep instead
+    const char* sweep = std::getenv("LCS_B200_FUSED_SWEEP");
+    use_tma = std::is_same<T, double>::value && c.coloring == LCS_COLORING_RED_BLACK_FAST &&
+              !(sweep && std::string(sweep) == "plain");
+    if (use_tma) LCS_TRY(init_tma());
     LCS_CUDA(cudaStreamSynchronize(stream));
     return LCS_OK;
   }
+
+  // ---------------------------------------------------------- tensor maps
+  static constexpr int TNS = 4;
+  bool use_tma = false;
+  TensorMaps tmaps;
+  // tile shape of the TMA sweep: 0 = 64x8, 1 = 32x16, 2 = 32x8, 3 = 64x16
+  // (LCS_B200_TILE=64x8|32x16|32x8|64x16); LCS_B200_ZCHUNK forces the z chunk
+  int tile_variant = 0, zchunk_force = 0, TTX = 64, TTY = 8;
+  size_t tma_smem = 0;
+  const void* tma_fn = nullptr;
+  int init_tma() {
+    if (const char* t = std::getenv("LCS_B200_TILE")) {
+      const std::string v(t);
+      tile_variant = v == "32x16" ? 1 : v == "32x8" ? 2 : v == "64x16" ? 3 : 0;
+    }
+    if (const char* z = std::getenv("LCS_B200_ZCHUNK")) zchunk_force = std::atoi(z);
+    switch (tile_variant) {
+      case 1: TTX = 32; TTY = 16; tma_smem = TmaLayout<32, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 16, TNS>; break;
+      case 2: TTX = 32; TTY = 8; tma_smem = TmaLayout<32, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 8, TNS>; break;
+      case 3: TTX = 64; TTY = 16; tma_smem = TmaLayout<64, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<64, 16, TNS>; break;
+      default: TTX = 64; TTY = 8; tma_smem = TmaLayout<64, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<64, 8, TNS>; break;
+    }
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    LCS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled is unavailable");
+    auto encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)(g.n[1] + 2 * g.h), (cuuint64_t)(g.n[2] + 2 * g.h)};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.pz * sizeof(T)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const cuuint32_t vbox[3] = {(cuuint32_t)TTX + 4, (cuuint32_t)TTY + 4, 1};
+    const cuuint32_t pbox[3] = {(cuuint32_t)TTX, (cuuint32_t)TTY, 1};
+    for (int b = 0; b < kVelMaps; b++) {
+      CUresult r = encode(&tmaps.vel[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, vel0[b / 3][b % 3], dims, strides, vbox,
+                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (velocity %d) failed: %d", b, (int)r);
+    }
+    CUresult r = encode(&tmaps.P, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)P, dims, strides, pbox, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (P) failed: %d", (int)r);
+    LCS_CUDA(cudaFuncSetAttribute(tma_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem));
+    LCS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, cfg.device));
+    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_ctas_per_sm, tma_fn, (TTX / 2) * TTY, tma_smem));
+    if (tma_ctas_per_sm < 1) return fail(LCS_ECUDA, "the TMA sweep does not fit on an SM");
+    return LCS_OK;
+  }
+  int num_sms = 148, tma_ctas_per_sm = 1;
 
   int init_rcf() {
     const int cs = cfg.coarse_size;
@@ -392,6 +455,7 @@ class Engine : public EngineBase {
     return f;
   }
   int fused(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks = nullptr) {
+    if (use_tma) return fused_tma(set, D, out, fill_r, part, finalize, group_end, nblocks);
     const FusedGeom f = fused_geom(out);
     const int64_t nb = (int64_t)f.gx * f.gy * f.gz;
     if (nb > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
@@ -399,6 +463,43 @@ class Engine : public EngineBase {
     return launch("hsmac_fused", k_hsmac_fused<T, TX, TY>, dim3(f.gx, f.gy, f.gz), dim3(TX * TY), 0, dctx, g, set, P, D,
                   out, f.gb, fill_r, f.zchunk, hc, part, finalize, group_end, 1);
   }
+  // TMA-fed sweep: the periodic fill first (in place, like synchalo!), then
+  // one pass over tiles whose first column is odd (16-byte TMA rule)
+  int fused_tma(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
+    if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
+    const Box gb = bbox(out, cube(g, 1, 0));
+    const int xo = (gb.lo[0] & 1) ? gb.lo[0] : gb.lo[0] - 1;
+    const int gx = (gb.hi[0] - xo + 1 + TTX - 1) / TTX, gy = (gb.len(1) + TTY - 1) / TTY;
+    // z chunks: minimise (waves of resident CTAs) x (planes per chunk + the 4
+    // warm-up/drain planes a chunk costs)
+    const int nzc = gb.len(2), ncols = gx * gy, slots = num_sms * tma_ctas_per_sm;
+    int best_nc = 1;
+    double best = 1e300;
+    for (int nc = 1; nc <= std::min(nzc, 64); nc++) {
+      const int zc = (nzc + nc - 1) / nc;
+      const int nch = (nzc + zc - 1) / zc;
+      const int64_t items = (int64_t)ncols * nch;
+      const double waves = std::ceil((double)items / slots);
+      const double cost = waves * (zc + 4);
+      if (cost < best - 1e-9) { best = cost; best_nc = nc; }
+    }
+    const int zc = zchunk_force > 0 ? std::min(zchunk_force, nzc) : (nzc + best_nc - 1) / best_nc;
+    const int nitems = ncols * ((nzc + zc - 1) / zc);
+    if (nitems > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
+    if (nblocks) *nblocks = nitems;
+    const dim3 grid(nitems), block((TTX / 2) * TTY);
+    switch (tile_variant) {
+      case 1: return launch("hsmac_tma", k_hsmac_tma<32, 16, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
+                            (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+      case 2: return launch("hsmac_tma", k_hsmac_tma<32, 8, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
+                            (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+      case 3: return launch("hsmac_tma", k_hsmac_tma<64, 16, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
+                            (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+      default: return launch("hsmac_tma", k_hsmac_tma<64, 8, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
+                             (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+    }
+  }
+
   // in-place colour phases over a box (both colours), partial sums appended
   int phases(int set, Box b, double* part, int* used) {
     if (b.lo[0] > b.hi[0] || b.lo[1] > b.hi[1] || b.lo[2] > b.hi[2]) return LCS_OK;
@@ -514,6 +615,7 @@ class Engine : public EngineBase {
       const int last_itr_in_group = itr + spg - 1;
       if (last_itr_in_group >= cfg.itrmin) {
         LCS_TRY(read_ctx());
+        if (hctx->tma_error) return fail(LCS_ETIMEDOUT, "a bounded wait on a TMA tile load ran out");
         if (hctx->nonfinite) return fail(LCS_ENONFINITE, "HSMAC residual is not finite");
         if (hctx->cs.done) break;
         itr = hctx->cs.itr;
@@ -838,6 +940,7 @@ class Engine : public EngineBase {
     }
     LCS_TRY(collect_profile());
     LCS_TRY(read_ctx());
+    if (hctx->tma_error) return fail(LCS_ETIMEDOUT, "a bounded wait on a TMA tile load ran out");
     if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt");
     if (log) fill_log(hctx->cur, log);
     return LCS_OK;
@@ -880,6 +983,7 @@ class Engine : public EngineBase {
         if (e1 && q == nsteps - 1) LCS_CUDA(cudaEventRecord(e1, stream));
         LCS_TRY(collect_profile());
         LCS_TRY(read_ctx());
+        if (hctx->tma_error) return fail(LCS_ETIMEDOUT, "a bounded wait on a TMA tile load ran out");
         if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt at step %lld", (long long)hctx->step);
         if (logs) fill_log(hctx->cur, &logs[q]);
       }
@@ -896,6 +1000,7 @@ class Engine : public EngineBase {
       }
       if (e1 && done + chunk == nsteps) LCS_CUDA(cudaEventRecord(e1, stream));
       LCS_TRY(read_ctx());
+      if (hctx->tma_error) return fail(LCS_ETIMEDOUT, "a bounded wait on a TMA tile load ran out");
       if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt near step %lld", (long long)hctx->step);
       if (logs) {
         std::vector<StepLog> hl(chunk);

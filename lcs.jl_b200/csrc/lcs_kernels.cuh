@@ -54,7 +54,7 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
 template <int NT>
 __device__ __forceinline__ double sum_partials(const double* partials, int n, double* sh) {
   double v = 0.0;
-  for (int q = threadIdx.x; q < n; q += NT) v += partials[q];
+  for (int q = threadIdx.x; q < n; q += NT) v += __ldcg(&partials[q]);
   return block_sum<NT>(v, sh);
 }
 
@@ -576,6 +576,9 @@ __global__ void __launch_bounds__(TX * TY) k_hsmac_fused(Ctx* __restrict__ ctx, 
           void* tmp = ctx->vel[set][c];
           ctx->vel[set][c] = ctx->vel[kSetSpare][c];
           ctx->vel[kSetSpare][c] = tmp;
+          const int tp = ctx->vphys[set][c];
+          ctx->vphys[set][c] = ctx->vphys[kSetSpare][c];
+          ctx->vphys[kSetSpare][c] = tp;
         }
     }
   }

@@ -64,10 +64,18 @@ def test_update_and_fused_rhs_update_bitwise(stage):
 VARIANTS = [(tb, ov) for tb in (True, False) for ov in (True, False)]
 
 
+@pytest.fixture(params=["tma", "plain"])
+def sweep(request, monkeypatch):
+    """Both implementations of the fused red-black sweep: the TMA-fed one
+    (default for red-black-fast) and the plain-load one."""
+    monkeypatch.setenv("LCS_B200_FUSED_SWEEP", request.param)
+    return request.param
+
+
 @pytest.mark.parametrize("tb,ov", VARIANTS)
 @pytest.mark.parametrize("coloring,block", [(F.COLORING_RED_BLACK_FAST, 0), (F.COLORING_RED_BLACK, 0),
                                             (F.COLORING_RED_BLACK_BLOCK, 2)])
-def test_hsmac_reference_setting_bitwise(tb, ov, coloring, block):
+def test_hsmac_reference_setting_bitwise(tb, ov, coloring, block, sweep):
     """The reference's couple test: 16^3, h=3, omega 1.7, epsp 1e-3, itrmin = itrmax = 6,
     random haloed U, V, W, P (test/test_flows.jl:82-101)."""
     cfg = make_config(16, mode=F.MODE_FLOW, time_blocking=tb, overlap=ov, coloring=coloring, block=block)
@@ -82,7 +90,7 @@ def test_hsmac_reference_setting_bitwise(tb, ov, coloring, block):
 
 @pytest.mark.parametrize("tb,ov", VARIANTS)
 @pytest.mark.parametrize("n,epsp", [(34, 2e-2), (64, 2e-2), (34, 1e3)])
-def test_hsmac_long_runs_and_early_exit(tb, ov, n, epsp):
+def test_hsmac_long_runs_and_early_exit(tb, ov, n, epsp, sweep):
     """Partial tiles (n = 34), several z chunks (n = 64), a data-dependent exit,
     and an exit at exactly itrmin (epsp = 1e3)."""
     cfg = make_config(n, mode=F.MODE_FLOW, time_blocking=tb, overlap=ov, itrmin=6, itrmax=60, epsp=epsp)
@@ -101,6 +109,28 @@ def test_hsmac_long_runs_and_early_exit(tb, ov, n, epsp):
         assert lg["itr"] == 6 and lg["sweeps"] == 7
     assert abs(lg["div"] - lo["div"]) <= 1e-12 * lo["div"]
     same_fields(g, o, fs)
+
+
+@pytest.mark.parametrize("tb,ov", VARIANTS)
+def test_tma_sweep_equals_plain_sweep_128(tb, ov, monkeypatch):
+    """At 128^3 (several tiles and z chunks per sweep) the TMA-fed and the
+    plain-load fused sweeps give identical fields."""
+    from lcs_b200 import inits
+
+    out = []
+    for mode in ("tma", "plain"):
+        monkeypatch.setenv("LCS_B200_FUSED_SWEEP", mode)
+        e = Engine(make_config(128, mode=F.MODE_FLOW, time_blocking=tb, overlap=ov, itrmin=6, itrmax=12,
+                               epsp=1e-12))
+        U, V, W, P = inits.spectral_flow(128, seed=4)
+        e.upload_flow(U, V, W, P)
+        lg = e.couple(2, 0.003)
+        out.append((lg, e.download_flow()))
+        e.close()
+    (la, fa), (lb, fb) = out
+    assert la["itr"] == lb["itr"] and abs(la["div"] - lb["div"]) <= 1e-13 * lb["div"]
+    for a, b in zip(fa, fb):
+        assert np.array_equal(a, b)
 
 
 def test_synchalo_bitwise():
@@ -241,7 +271,7 @@ def evolve_pair(cfg, steps, seed=0, nparts=(2000,), graphs=False):
 
 @pytest.mark.parametrize("forcing", [F.FORCING_LINEAR_POWER, F.FORCING_RC_ENERGY])
 @pytest.mark.parametrize("graphs", [False, True])
-def test_ten_steps_rel_l2(forcing, graphs):
+def test_ten_steps_rel_l2(forcing, graphs, sweep):
     """North-star parity: fields rel-L2 <= 1e-10 after 10 steps (config-0 style)."""
     cfg = make_config(32, forcing=forcing, power=0.5, energy=0.649, kmin=1, kmax=2, coarse=8, Re=100.0,
                       itrmin=6, itrmax=40, epsp=1e-8 * 2 * math.pi / 32, graphs=int(graphs),

@@ -56,6 +56,11 @@ WORKLOADS = {
                   precision="fp64"),
 }
 
+# DRAM bytes (read + write) per launch of the sweep kernel, per interior cell,
+# from one `ncu --set full` capture of `python bench.py --steps 1 --warmup 0
+# --no-cpu-baseline` (rc256); filled in per kernel once it has been captured.
+SWEEP_DRAM_BYTES_PER_CELL = {}
+
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -271,12 +276,16 @@ def run_b200(args):
     # kernel launches per step, counted on the launch-by-launch (profiled) path;
     # the graph replays the same kernels with the same loop counts
     launches = int(round(sum(v[1] for v in tot.values()) / prof_steps * args.steps))
-    ms_fused, cnt = tot.get("hsmac_fused", (0.0, 0))
+    # the dominant kernel: the fused red-black sweep (TMA-fed, or the plain form)
+    sweep_kernel = max(("hsmac_tma", "hsmac_fused"), key=lambda k: tot.get(k, (0.0, 0))[0])
+    ms_sweep, cnt = tot.get(sweep_kernel, (0.0, 0))
     T = 8
     peak, peak_kind = hbm_peak()
     alg_bytes = 8 * T * n3  # U, V, W, P read and written once per interior cell per sweep
-    avg_ms = ms_fused / max(cnt, 1)
+    avg_ms = ms_sweep / max(cnt, 1)
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9 if cnt else None
+    traffic = SWEEP_DRAM_BYTES_PER_CELL.get(sweep_kernel)
+    traffic = traffic * n3 if traffic else None
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in sorted(tot.items(), key=lambda kv: -kv[1][0])}
 
     # end to end through the public API: pinned host state in, the per-step
@@ -325,9 +334,10 @@ def run_b200(args):
             "hsmac_sweeps_per_step": statistics.mean(sweeps) if sweeps else None,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
-            "roofline": {"kernel": "hsmac_fused", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "roofline": {"kernel": sweep_kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": None, "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
+                         "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum",
+                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
             "kernels": kernels,
             "e2e": {"value": e2e_value, "unit": "Mcell-steps/s",
                     "h2d_bytes_per_step": (h2d1 - h2d0) / e2e_steps, "d2h_bytes_per_step": (d2h1 - d2h0) / e2e_steps,

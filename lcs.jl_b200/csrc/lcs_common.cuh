@@ -95,7 +95,8 @@ struct Ctx {
   StepLog cur;          // log of the step in progress
   unsigned int ticket;  // last-block-done counter
   int nonfinite;        // sticky: a NaN/Inf dt or residual was seen
-  int tma_error;        // sticky: a bounded wait on a TMA copy ran out
+  int wait_error;       // sticky: a bounded device wait (TMA copy, grid barrier) ran out
+  unsigned int gbar_count, gbar_gen;  // grid-wide barrier of cooperative kernels
 };
 
 // ---- stencil primitives (src/diff.jl:1-39), same evaluation order --------

@@ -260,6 +260,7 @@ class Engine : public EngineBase {
     use_tma = std::is_same<T, double>::value && c.coloring == LCS_COLORING_RED_BLACK_FAST &&
               !(sweep && std::string(sweep) == "plain");
     if (use_tma) LCS_TRY(init_tma());
+    LCS_TRY(init_faces());
     LCS_CUDA(cudaStreamSynchronize(stream));
     return LCS_OK;
   }
@@ -312,6 +313,19 @@ class Engine : public EngineBase {
     return LCS_OK;
   }
   int num_sms = 148, tma_ctas_per_sm = 1;
+
+  // blocks of the cooperative face-phase kernel (0: twelve in-place launches)
+  int face_grid = 0;
+  int init_faces() {
+    int coop = 0, per_sm = 0;
+    LCS_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, cfg.device));
+    LCS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, cfg.device));
+    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hsmac_faces<T>, 256, 0));
+    const char* f = std::getenv("LCS_B200_FACES");
+    const bool sequential = f && std::string(f) == "phases";
+    face_grid = (coop && per_sm > 0 && !sequential) ? std::min(per_sm, 2) * num_sms : 0;
+    return LCS_OK;
+  }
 
   int init_rcf() {
     const int cs = cfg.coarse_size;
@@ -369,6 +383,35 @@ class Engine : public EngineBase {
     }
     kernel<<<grid, block, smem, stream>>>(args...);
     cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(LCS_ECUDA, "launch %s: %s", label, cudaGetErrorString(e));
+    if (a) {
+      cudaEventRecord(b, stream);
+      recs.push_back({label, a, b});
+    }
+    launches++;
+    return LCS_OK;
+  }
+  // launch whose blocks are all co-resident (they meet at grid barriers)
+  template <typename... P, typename... A>
+  int launch_coop(const char* label, void (*kernel)(P...), dim3 grid, dim3 block, A... args) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (prof && !capturing) {
+      a = get_event();
+      b = get_event();
+      cudaEventRecord(a, stream);
+    }
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = grid;
+    lc.blockDim = block;
+    lc.dynamicSmemBytes = 0;
+    lc.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&lc, kernel, args...);
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return fail(LCS_ECUDA, "launch %s: %s", label, cudaGetErrorString(e));
     if (a) {
       cudaEventRecord(b, stream);
@@ -552,6 +595,14 @@ class Engine : public EngineBase {
     }
     Box f[6];
     faces_of(dom, core, f);
+    const bool core_nonempty = core.len(0) > 0 && core.len(1) > 0 && core.len(2) > 0;
+    if (face_grid > 0 && core_nonempty && cfg.coloring != LCS_COLORING_RED_BLACK_BLOCK &&
+        used + face_grid <= plan.partials_cap) {
+      FaceSet fs;
+      for (int q = 0; q < 6; q++) fs.f[q] = f[q];
+      return launch_coop("hsmac_faces", k_hsmac_faces<T>, dim3(face_grid), dim3(256), dctx, g, set, P, fs, hc,
+                         partials, used, group_end);
+    }
     for (int q = 0; q < 6; q++) LCS_TRY(phases(set, f[q], partials, &used));
     return finalize_sweep(used, group_end);
   }
@@ -615,7 +666,7 @@ class Engine : public EngineBase {
       const int last_itr_in_group = itr + spg - 1;
       if (last_itr_in_group >= cfg.itrmin) {
         LCS_TRY(read_ctx());
-        if (hctx->tma_error) return fail(LCS_ETIMEDOUT, "a bounded wait on a TMA tile load ran out");
+        if (hctx->wait_error) return fail(LCS_ETIMEDOUT, "a bounded device wait (TMA tile load or grid barrier) ran out");
         if (hctx->nonfinite) return fail(LCS_ENONFINITE, "HSMAC residual is not finite");
         if (hctx->cs.done) break;
         itr = hctx->cs.itr;
@@ -940,7 +991,7 @@ class Engine : public EngineBase {
     }
     LCS_TRY(collect_profile());
     LCS_TRY(read_ctx());
-    if (hctx->tma_error) return fail(LCS_ETIMEDOUT, "a bounded wait on a TMA tile load ran out");
+    if (hctx->wait_error) return fail(LCS_ETIMEDOUT, "a bounded device wait (TMA tile load or grid barrier) ran out");
     if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt");
     if (log) fill_log(hctx->cur, log);
     return LCS_OK;
@@ -983,7 +1034,7 @@ class Engine : public EngineBase {
         if (e1 && q == nsteps - 1) LCS_CUDA(cudaEventRecord(e1, stream));
         LCS_TRY(collect_profile());
         LCS_TRY(read_ctx());
-        if (hctx->tma_error) return fail(LCS_ETIMEDOUT, "a bounded wait on a TMA tile load ran out");
+        if (hctx->wait_error) return fail(LCS_ETIMEDOUT, "a bounded device wait (TMA tile load or grid barrier) ran out");
         if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt at step %lld", (long long)hctx->step);
         if (logs) fill_log(hctx->cur, &logs[q]);
       }
@@ -1000,7 +1051,7 @@ class Engine : public EngineBase {
       }
       if (e1 && done + chunk == nsteps) LCS_CUDA(cudaEventRecord(e1, stream));
       LCS_TRY(read_ctx());
-      if (hctx->tma_error) return fail(LCS_ETIMEDOUT, "a bounded wait on a TMA tile load ran out");
+      if (hctx->wait_error) return fail(LCS_ETIMEDOUT, "a bounded device wait (TMA tile load or grid barrier) ran out");
       if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt near step %lld", (long long)hctx->step);
       if (logs) {
         std::vector<StepLog> hl(chunk);

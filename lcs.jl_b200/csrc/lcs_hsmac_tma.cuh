@@ -10,11 +10,13 @@
 //  - every thread owns an x-pair of cells, one of each colour, so both colour
 //    phases keep all lanes busy (no red-black divergence);
 //  - writes are 16-byte stores of a pair; P is updated in place.
-// Waits on the mbarriers are bounded; a wait that runs out sets ctx->tma_error
+// Waits on the mbarriers are bounded; a wait that runs out sets ctx->wait_error
 // and the kernel stops computing (the host reports LCS_ETIMEDOUT).
 #pragma once
 
 #include <cuda.h>
+
+#include <type_traits>
 
 #include "lcs_common.cuh"
 
@@ -73,7 +75,9 @@ struct TmaLayout {
   static constexpr int DW = TX + 3, DH = TY + 3;  // dp of cells x0-1 .. x0+TX+1
   static constexpr size_t vel_bytes = (size_t)NS * 3 * VEL_TILE * 8;
   static constexpr size_t p_bytes = (size_t)NS * P_TILE * 8;
-  static constexpr size_t dp_bytes = (size_t)3 * DW * DH * 8;
+  // the dp ring sits between the velocity and P rings: the mask-free path of
+  // full tiles reads (and discards) neighbours up to a row beyond it
+  static constexpr size_t dp_bytes = ((size_t)3 * DW * DH * 8 + 127) / 128 * 128;
   static constexpr size_t bar_bytes = 8 * NS;
   static constexpr size_t red_bytes = 8 * 32;
   static constexpr size_t total = vel_bytes + p_bytes + dp_bytes + bar_bytes + red_bytes + 16;
@@ -130,8 +134,8 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
   constexpr int VW = L::VW, DW = L::DW, VT = L::VEL_TILE, DP = L::DW * L::DH;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* svel = (double*)smem_raw;                                 // [NS][3][VH][VW]
-  double* sP = (double*)(smem_raw + L::vel_bytes);                  // [NS][TY][TX]
-  double* sdp = (double*)(smem_raw + L::vel_bytes + L::p_bytes);    // [3][DH][DW]
+  double* sdp = (double*)(smem_raw + L::vel_bytes);                 // [3][DH][DW]
+  double* sP = (double*)(smem_raw + L::vel_bytes + L::dp_bytes);    // [NS][TY][TX]
   uint64_t* bars = (uint64_t*)(smem_raw + L::vel_bytes + L::p_bytes + L::dp_bytes);
   double* red = (double*)(smem_raw + L::vel_bytes + L::p_bytes + L::dp_bytes + L::bar_bytes);
   int* last_flag = (int*)(red + 32);
@@ -237,12 +241,20 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
       const int64_t o_g0 = g.at(oi, oj, 0);
       const int oij = oi + oj;
 
+      // A tile whose neighbourhood lies inside D (x, y), whose outputs lie inside
+      // `out` and whose cells are interior (x, y) needs no per-cell masks.
+      const bool full = x0 - 3 >= D.lo[0] && x0 + TX + 3 <= D.hi[0] && y0 - 2 >= D.lo[1] &&
+                        y0 + TY + 2 <= D.hi[1] && x0 >= out.lo[0] && x0 + TX - 1 <= out.hi[0] &&
+                        y0 >= out.lo[1] && y0 + TY - 1 <= out.hi[1] && x0 >= 1 && x0 + TX - 1 <= nx && y0 >= 1 &&
+                        y0 + TY - 1 <= ny;
+      auto sweep_planes = [&](auto full_tag) {
+      constexpr bool FULL = decltype(full_tag)::value;
       for (int l = 0; l < nplanes; l++) {
         const int s = kb - 2 + l;
         const int li = load0 + l;
         const int slot = li % NS;
         if (!mbar_wait_bounded(&bars[slot], (uint32_t)((li / NS) & 1))) {
-          ctx->tma_error = 1;
+          ctx->wait_error = 1;
           ok = false;
         }
         if (__syncthreads_or(!ok)) {
@@ -275,11 +287,12 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
           const int dx = it_dx[rd] + o;
           const int sx = it_vrow[rd] + dx + 1;
           const int dofs = it_drow[rd] + dx;
-          const bool mxy = ((b >> (o + 1)) & 1u) && ((b >> 5) & 1u);
+          const bool mxy = FULL || (((b >> (o + 1)) & 1u) && ((b >> 5) & 1u));
           const bool inside = (b >> (13 + o)) & 1u;
           const bool own = ((b >> (10 + o)) & 1u) && ((b >> 12) & 1u);
           double dp0 = 0.0;
-          const bool m0 = do0 && inside && z_s && mxy;
+          // (FULL: the cell beyond the dp region is computed and not stored)
+          const bool m0 = do0 && z_s && (FULL || (inside && mxy));
           if (m0) {
             const double dudx = dxi * (-Us[sx - 1] + Us[sx]);
             const double dvdy = dyi * (-Vs[sx - VW] + Vs[sx]);
@@ -290,24 +303,25 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
           }
           if (do0 && inside) d_s[dofs] = dp0;
           // dp1 at (same i, j, plane s-1)
-          if (do1 && z_m && mxy && ((b >> (7 + o)) & 1u) && ((b >> 9) & 1u)) {
+          const bool in1 = ((b >> (7 + o)) & 1u) && ((b >> 9) & 1u);  // inside the dp1 region
+          if (do1 && z_m && (FULL || (mxy && in1))) {
             double ul = Um[sx - 1], ur = Um[sx];
             double vl = Vm[sx - VW], vr = Vm[sx];
             double wl = Wb[sx], wr = Wm[sx];
             const double cl = d_m[dofs - 1] * dxi, cr = d_m[dofs + 1] * dxi;
             const double cd = d_m[dofs - DW] * dyi, cu = d_m[dofs + DW] * dyi;
             const double cb = d_b[dofs] * dzi, ct = dp0 * dzi;
-            ul = ((b >> o) & 1u) ? ul + cl : ul;
-            ur = ((b >> (o + 2)) & 1u) ? ur - cr : ur;
-            vl = ((b >> 4) & 1u) ? vl + cd : vl;
-            vr = ((b >> 6) & 1u) ? vr - cu : vr;
+            ul = (FULL || ((b >> o) & 1u)) ? ul + cl : ul;
+            ur = (FULL || ((b >> (o + 2)) & 1u)) ? ur - cr : ur;
+            vl = (FULL || ((b >> 4) & 1u)) ? vl + cd : vl;
+            vr = (FULL || ((b >> 6) & 1u)) ? vr - cu : vr;
             wl = z_b ? wl + cb : wl;
             wr = m0 ? wr - ct : wr;
             const double dudx = dxi * (-ul + ur);
             const double dvdy = dyi * (-vl + vr);
             const double dwdz = dzi * (-wl + wr);
             const double div = dudx + dvdy + dwdz;
-            d_m[dofs] = -om * div * dl;
+            if (!FULL || in1) d_m[dofs] = -om * div * dl;
             if (own_m && own) racc += div * div;
           }
         }
@@ -317,22 +331,22 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
         const bool lower_first1 = ((oij + k1) & 1) == 0;  // cell oi is colour 0 at k1
         if (k1 >= kb && k1 <= ke) {
           const double dA = d_m[o_dofs], dB = d_m[o_dofs + 1], dC = d_m[o_dofs + 2];
-          const bool mA = z_m && ((ob >> 0) & 1u) && ((ob >> 3) & 1u);
-          const bool mB = z_m && ((ob >> 1) & 1u) && ((ob >> 3) & 1u);
-          const bool mC = z_m && ((ob >> 2) & 1u) && ((ob >> 3) & 1u);
-          const bool yup = z_m && ((ob >> 4) & 1u);
+          const bool mA = z_m && (FULL || (((ob >> 0) & 1u) && ((ob >> 3) & 1u)));
+          const bool mB = z_m && (FULL || (((ob >> 1) & 1u) && ((ob >> 3) & 1u)));
+          const bool mC = z_m && (FULL || (((ob >> 2) & 1u) && ((ob >> 3) & 1u)));
+          const bool yup = z_m && (FULL || ((ob >> 4) & 1u));
           // cell oi (colour c0) and oi+1 (colour 1-c0)
           const double u0 = face_update(Um[o_vofs], lower_first1, mA, dA, mB, dB, dxi);
           const double u1 = face_update(Um[o_vofs + 1], !lower_first1, mB, dB, mC, dC, dxi);
-          const double v0 = face_update(Vm[o_vofs], lower_first1, mA, dA, yup && ((ob >> 0) & 1u),
+          const double v0 = face_update(Vm[o_vofs], lower_first1, mA, dA, yup && (FULL || ((ob >> 0) & 1u)),
                                         d_m[o_dofs + DW], dyi);
-          const double v1 = face_update(Vm[o_vofs + 1], !lower_first1, mB, dB, yup && ((ob >> 1) & 1u),
+          const double v1 = face_update(Vm[o_vofs + 1], !lower_first1, mB, dB, yup && (FULL || ((ob >> 1) & 1u)),
                                         d_m[o_dofs + 1 + DW], dyi);
           const double p0o = sP[slm * L::P_TILE + o_pofs], p1o = sP[slm * L::P_TILE + o_pofs + 1];
           const double p0 = mA ? p0o + dA * dti : p0o;
           const double p1 = mB ? p1o + dB * dti : p1o;
-          const bool oy = ((ob >> 7) & 1u) && k1 >= out.lo[2] && k1 <= out.hi[2];
-          const bool oa = oy && ((ob >> 5) & 1u), obb = oy && ((ob >> 6) & 1u);
+          const bool oy = (FULL || ((ob >> 7) & 1u)) && k1 >= out.lo[2] && k1 <= out.hi[2];
+          const bool oa = oy && (FULL || ((ob >> 5) & 1u)), obb = oy && (FULL || ((ob >> 6) & 1u));
           const int64_t o = o_g0 + (int64_t)k1 * g.pz;
           if (oa && obb) {
             *(double2*)(Uo + o) = make_double2(u0, u1);
@@ -342,8 +356,8 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
             if (obb) { Uo[o + 1] = u1; Vo[o + 1] = v1; }
           }
           // P in place on the interior only (P halos are refilled before any read)
-          const bool pj = k1 >= 1 && k1 <= nz && ((ob >> 10) & 1u);
-          const bool pa = pj && ((ob >> 8) & 1u), pb = pj && ((ob >> 9) & 1u);
+          const bool pj = k1 >= 1 && k1 <= nz && (FULL || ((ob >> 10) & 1u));
+          const bool pa = pj && (FULL || ((ob >> 8) & 1u)), pb = pj && (FULL || ((ob >> 9) & 1u));
           if (pa && pb) {
             *(double2*)(P + o) = make_double2(p0, p1);
           } else {
@@ -353,13 +367,14 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
         }
         if (k2 >= kb && k2 <= ke) {
           // W face between planes k2 and k1 = k2+1; cell oi at k2 has colour 1-c0(k1)
-          const bool mxA = ((ob >> 0) & 1u) && ((ob >> 3) & 1u), mxB = ((ob >> 1) & 1u) && ((ob >> 3) & 1u);
+          const bool mxA = FULL || (((ob >> 0) & 1u) && ((ob >> 3) & 1u));
+          const bool mxB = FULL || (((ob >> 1) & 1u) && ((ob >> 3) & 1u));
           const double w0 = face_update(Wb[o_vofs], !lower_first1, z_b && mxA, d_b[o_dofs], z_m && mxA,
                                         d_m[o_dofs], dzi);
           const double w1 = face_update(Wb[o_vofs + 1], lower_first1, z_b && mxB, d_b[o_dofs + 1], z_m && mxB,
                                         d_m[o_dofs + 1], dzi);
-          const bool oy = ((ob >> 7) & 1u) && k2 >= out.lo[2] && k2 <= out.hi[2];
-          const bool oa = oy && ((ob >> 5) & 1u), obb = oy && ((ob >> 6) & 1u);
+          const bool oy = (FULL || ((ob >> 7) & 1u)) && k2 >= out.lo[2] && k2 <= out.hi[2];
+          const bool oa = oy && (FULL || ((ob >> 5) & 1u)), obb = oy && (FULL || ((ob >> 6) & 1u));
           const int64_t o = o_g0 + (int64_t)k2 * g.pz;
           if (oa && obb) {
             *(double2*)(Wo + o) = make_double2(w0, w1);
@@ -370,6 +385,12 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
         }
         __syncthreads();
         if (tid == 0 && l + NS - 2 < nplanes) issue(l + NS - 2);
+      }
+      };
+      if (full) {
+        sweep_planes(std::true_type{});
+      } else {
+        sweep_planes(std::false_type{});
       }
     }
     if (!ok) {
@@ -385,10 +406,10 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
   const unsigned int bid = blockIdx.x;
   if (tid == 0) partials[bid] = bs;
   if (last_block(&ctx->ticket, nb, last_flag)) {
-    if (skip || ctx->tma_error) {
+    if (skip || ctx->wait_error) {
       if (tid == 0) {
         ctx->ticket = 0;
-        if (ctx->tma_error) ctx->cs.done = 1;
+        if (ctx->wait_error) ctx->cs.done = 1;
       }
       return;
     }

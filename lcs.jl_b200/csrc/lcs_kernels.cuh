@@ -370,6 +370,153 @@ __global__ void __launch_bounds__(256) k_hsmac_finalize(Ctx* ctx, const double* 
   if (threadIdx.x == 0) hsmac_check(ctx, cf, s, group_end);
 }
 
+// --------------------------------------------------------------------------
+// grid-wide barrier of a cooperative launch (all blocks co-resident), with a
+// bounded wait: false when the generation did not advance within the limit.
+// --------------------------------------------------------------------------
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+constexpr int kGridBarrierSpins = 1 << 22;  // x >= 32 ns sleeps: > 0.1 s
+
+__device__ __forceinline__ bool grid_barrier(Ctx* ctx, unsigned int nblocks, int* flag_sh) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned int gen = ld_acquire_gpu(&ctx->gbar_gen);
+    __threadfence();  // the block's writes (ordered by the __syncthreads) before the arrival
+    if (atomicAdd(&ctx->gbar_count, 1u) == nblocks - 1) {
+      ctx->gbar_count = 0;
+      __threadfence();
+      atomicAdd(&ctx->gbar_gen, 1u);
+    } else {
+      int it = 0;
+      while (ld_acquire_gpu(&ctx->gbar_gen) == gen) {
+        if (++it > kGridBarrierSpins) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    *flag_sh = ok;
+  }
+  __syncthreads();
+  return *flag_sh != 0;
+}
+
+// The six face slabs of an overlap sweep (Topologies.faces, halo.jl:349-366),
+// in the reference's order: z-low, z-high, y-low, y-high, x-low, x-high.
+struct FaceSet {
+  Box f[6];
+};
+
+// In-place colour phase of one face slab for the cell with flat index t among
+// the colour's cells (the k_hsmac_phase mapping); returns whether a cell was
+// updated and its div in *div.  Loads bypass L1 (__ldcg): after a grid
+// barrier a block reads cells that other blocks have just written.
+template <typename T>
+__device__ __forceinline__ bool face_cell(const Grid& g, const Box& b, int64_t t, int color, int coloring, T* U, T* V,
+                                          T* W, T* P, T dxi, T dyi, T dzi, T dl, T om, T dti, T* div_out, bool* in_r) {
+  const int lx = b.len(0), ly = b.len(1);
+  const int hx = (lx + 1) / 2;
+  int64_t u = t;
+  const int m = (int)(u % hx); u /= hx;
+  const int j = b.lo[1] + (int)(u % ly); u /= ly;
+  const int k = b.lo[2] + (int)u;
+  const int a = b.lo[0];
+  const int i = a + 2 * m + ((j + k - a + color) & 1);
+  if (i > b.hi[0]) return false;
+  if (cell_color(coloring, i, j, k) != color) return false;
+  const int64_t c = g.at(i, j, k), sy = g.px, sz = g.pz;
+  const T u0 = __ldcg(U + c - 1), u1 = __ldcg(U + c);
+  const T v0 = __ldcg(V + c - sy), v1 = __ldcg(V + c);
+  const T w0 = __ldcg(W + c - sz), w1 = __ldcg(W + c);
+  const T p0 = __ldcg(P + c);
+  const T dudx = dxi * diff1_o2_at_half<T>(u0, u1);
+  const T dvdy = dyi * diff1_o2_at_half<T>(v0, v1);
+  const T dwdz = dzi * diff1_o2_at_half<T>(w0, w1);
+  const T div = dudx + dvdy + dwdz;
+  const T dp = -om * div * dl;
+  P[c] = p0 + dp * dti;
+  U[c - 1] = u0 - dp * dxi;
+  U[c] = u1 + dp * dxi;
+  V[c - sy] = v0 - dp * dyi;
+  V[c] = v1 + dp * dyi;
+  W[c - sz] = w0 - dp * dzi;
+  W[c] = w1 + dp * dzi;
+  *div_out = div;
+  *in_r = i >= 1 && i <= g.n[0] + 1 && j >= 1 && j <= g.n[1] + 1 && k >= 1 && k <= g.n[2] + 1;
+  return true;
+}
+
+// All face phases of one overlap sweep in one cooperative launch.  The
+// reference runs, after the core, colour 0 then colour 1 of each face in
+// turn (hsmac.jl:146-160).  Opposite faces never share a cell, a face value
+// or a P value (they are separated by the non-empty core), so each pair runs
+// as one phase: 3 pairs x 2 colours = 6 phases with a grid barrier between
+// them, the same in-place result as the twelve sequential launches.  Then
+// the block partials join the core sweep's partials[0, part0), and the last
+// block runs the exit test (k_hsmac_finalize's work).
+template <typename T>
+__global__ void __launch_bounds__(256) k_hsmac_faces(Ctx* __restrict__ ctx, Grid g, int set, T* __restrict__ P,
+                                                     FaceSet fs, HsmacCoef cf, double* __restrict__ partials,
+                                                     int part0, int group_end) {
+  __shared__ double sh[8];
+  __shared__ int flag;
+  if (ctx->cs.done) return;  // written before this launch: the same in every block
+  T* U = (T*)ctx->vel[set][0];
+  T* V = (T*)ctx->vel[set][1];
+  T* W = (T*)ctx->vel[set][2];
+  const T dxi = (T)cf.dxi, dyi = (T)cf.dyi, dzi = (T)cf.dzi, dl = (T)cf.dl, om = (T)cf.omega;
+  const T dti = (T)(1.0 / ctx->scal[0]);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double acc = 0.0;
+  bool ok = true;
+  for (int p = 0; p < 6; p++) {
+    const int color = p & 1;
+    const Box& ba = fs.f[p & ~1];
+    const Box& bb = fs.f[(p & ~1) + 1];
+    auto ncell = [](const Box& b) -> int64_t {
+      if (b.lo[0] > b.hi[0] || b.lo[1] > b.hi[1] || b.lo[2] > b.hi[2]) return 0;
+      return (int64_t)((b.len(0) + 1) / 2) * b.len(1) * b.len(2);
+    };
+    const int64_t na = ncell(ba), nt = na + ncell(bb);
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += stride) {
+      T div;
+      bool in_r;
+      const bool upd = t < na ? face_cell<T>(g, ba, t, color, cf.coloring, U, V, W, P, dxi, dyi, dzi, dl, om, dti,
+                                             &div, &in_r)
+                              : face_cell<T>(g, bb, t - na, color, cf.coloring, U, V, W, P, dxi, dyi, dzi, dl, om,
+                                             dti, &div, &in_r);
+      if (upd && in_r) acc += (double)div * (double)div;
+    }
+    if (p < 5 && !grid_barrier(ctx, gridDim.x, &flag)) {
+      if (threadIdx.x == 0) ctx->wait_error = 1;
+      ok = false;
+      break;
+    }
+  }
+  const double s = block_sum<256>(acc, sh);
+  if (threadIdx.x == 0) partials[part0 + blockIdx.x] = s;
+  if (last_block(&ctx->ticket, gridDim.x, &flag)) {
+    const double tot = sum_partials<256>(partials, part0 + (int)gridDim.x, sh);
+    if (threadIdx.x == 0) {
+      ctx->ticket = 0;
+      ctx->gbar_count = 0;  // every block has left its last barrier
+      if (ok && !ctx->wait_error) {
+        hsmac_check(ctx, cf, tot, group_end);
+      } else {
+        ctx->wait_error = 1;
+        ctx->cs.done = 1;
+      }
+    }
+  }
+}
+
 // Fused red-black sweep over the box D with the velocities ping-ponged:
 // reads set `set` (through an optional periodic halo fill of radius fill_r,
 // the synchalo! that precedes the sweep), writes the swept velocities into

@@ -24,6 +24,7 @@
 #include "lcs_base.h"
 #include "lcs_kernels.cuh"
 #include "lcs_hsmac_tma.cuh"
+#include "lcs_hsmac_rw.cuh"
 
 namespace lcs {
 
@@ -254,11 +255,13 @@ class Engine : public EngineBase {
     dc.with_particles = c.mode == LCS_MODE_FLOW_PARTICLE && c.n_species > 0;
     pc.dx = dx; pc.dy = dy; pc.dz = dz; pc.Re = Re;
     if (c.forcing == LCS_FORCING_RC_ENERGY) LCS_TRY(init_rcf());
-    // the TMA-fed sweep serves red-black-fast (the production colouring);
-    // LCS_B200_FUSED_SWEEP=plain selects the plain-load sweep instead
+    // the TMA-fed sweeps serve red-black-fast (the production colouring): the
+    // row-warp kernel by default; LCS_B200_FUSED_SWEEP=tma selects the
+    // thread-per-item TMA kernel, =plain the plain-load sweep
     const char* sweep = std::getenv("LCS_B200_FUSED_SWEEP");
-    use_tma = std::is_same<T, double>::value && c.coloring == LCS_COLORING_RED_BLACK_FAST &&
-              !(sweep && std::string(sweep) == "plain");
+    const std::string sw = sweep ? std::string(sweep) : std::string("rw");
+    use_tma = std::is_same<T, double>::value && c.coloring == LCS_COLORING_RED_BLACK_FAST && sw != "plain";
+    use_rw = use_tma && sw != "tma";
     if (use_tma) LCS_TRY(init_tma());
     LCS_TRY(init_faces());
     LCS_CUDA(cudaStreamSynchronize(stream));
@@ -271,7 +274,7 @@ class Engine : public EngineBase {
   TensorMaps tmaps;
   // tile shape of the TMA sweep: 0 = 64x8, 1 = 32x16, 2 = 32x8, 3 = 64x16
   // (LCS_B200_TILE=64x8|32x16|32x8|64x16); LCS_B200_ZCHUNK forces the z chunk
-  int tile_variant = 0, zchunk_force = 0, TTX = 64, TTY = 8;
+  int tile_variant = 0, zchunk_force = 0, TTX = 64, TTY = 8, tma_threads = 384;
   size_t tma_smem = 0;
   const void* tma_fn = nullptr;
   int init_tma() {
@@ -281,10 +284,14 @@ class Engine : public EngineBase {
     }
     if (const char* z = std::getenv("LCS_B200_ZCHUNK")) zchunk_force = std::atoi(z);
     switch (tile_variant) {
-      case 1: TTX = 32; TTY = 16; tma_smem = TmaLayout<32, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 16, TNS>; break;
-      case 2: TTX = 32; TTY = 8; tma_smem = TmaLayout<32, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 8, TNS>; break;
-      case 3: TTX = 64; TTY = 16; tma_smem = TmaLayout<64, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<64, 16, TNS>; break;
-      default: TTX = 64; TTY = 8; tma_smem = TmaLayout<64, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<64, 8, TNS>; break;
+      case 1: TTX = 32; TTY = 16; tma_smem = TmaLayout<32, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 16, TNS>;
+              tma_threads = TmaThreads<32, 16>::NT; break;
+      case 2: TTX = 32; TTY = 8; tma_smem = TmaLayout<32, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 8, TNS>;
+              tma_threads = TmaThreads<32, 8>::NT; break;
+      case 3: TTX = 64; TTY = 16; tma_smem = TmaLayout<64, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<64, 16, TNS>;
+              tma_threads = TmaThreads<64, 16>::NT; break;
+      default: TTX = 64; TTY = 8; tma_smem = TmaLayout<64, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<64, 8, TNS>;
+               tma_threads = TmaThreads<64, 8>::NT; break;
     }
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -306,13 +313,51 @@ class Engine : public EngineBase {
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (P) failed: %d", (int)r);
+    if (use_rw) {
+      // row-warp sweep: LCS_B200_RW=13 (tile rows, default) | 8 | 5
+      if (const char* v = std::getenv("LCS_B200_RW")) {
+        const std::string t(v);
+        rw_variant = t == "8" ? 1 : t == "5" ? 2 : 0;
+      }
+      switch (rw_variant) {
+        case 1: RTY = 8; rw_smem = RwLayout<8, 3>::total; rw_fn = (const void*)k_hsmac_rw<8, 3>;
+                rw_threads = RwLayout<8, 3>::NT; break;
+        case 2: RTY = 5; rw_smem = RwLayout<5, 3>::total; rw_fn = (const void*)k_hsmac_rw<5, 3>;
+                rw_threads = RwLayout<5, 3>::NT; break;
+        default: RTY = 13; rw_smem = RwLayout<13, 3>::total; rw_fn = (const void*)k_hsmac_rw<13, 3>;
+                 rw_threads = RwLayout<13, 3>::NT; break;
+      }
+      const cuuint32_t rbox[3] = {(cuuint32_t)RW_W, (cuuint32_t)RTY + 4, 1};
+      for (int b = 0; b < kVelMaps; b++) {
+        CUresult rr = encode(&tmaps_rw.vel[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, vel0[b / 3][b % 3], dims, strides,
+                             rbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (rr != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp velocity %d) failed: %d", b,
+                                            (int)rr);
+      }
+      const cuuint32_t rpbox[3] = {(cuuint32_t)RW_W, (cuuint32_t)RTY, 1};
+      CUresult rp = encode(&tmaps_rw.P, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)P, dims, strides, rpbox, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (rp != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp P) failed: %d", (int)rp);
+      LCS_CUDA(cudaFuncSetAttribute(rw_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
+    }
     LCS_CUDA(cudaFuncSetAttribute(tma_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem));
     LCS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, cfg.device));
-    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_ctas_per_sm, tma_fn, (TTX / 2) * TTY, tma_smem));
+    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_ctas_per_sm, tma_fn, tma_threads, tma_smem));
     if (tma_ctas_per_sm < 1) return fail(LCS_ECUDA, "the TMA sweep does not fit on an SM");
+    if (use_rw) {
+      LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rw_ctas_per_sm, rw_fn, rw_threads, rw_smem));
+      if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the row-warp sweep does not fit on an SM");
+    }
     return LCS_OK;
   }
   int num_sms = 148, tma_ctas_per_sm = 1;
+  bool use_rw = false;
+  TensorMaps tmaps_rw;
+  int rw_variant = 0, RTY = 13, rw_threads = 512, rw_ctas_per_sm = 1;
+  size_t rw_smem = 0;
+  const void* rw_fn = nullptr;
 
   // blocks of the cooperative face-phase kernel (0: twelve in-place launches)
   int face_grid = 0;
@@ -508,14 +553,9 @@ class Engine : public EngineBase {
   }
   // TMA-fed sweep: the periodic fill first (in place, like synchalo!), then
   // one pass over tiles whose first column is odd (16-byte TMA rule)
-  int fused_tma(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
-    if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
-    const Box gb = bbox(out, cube(g, 1, 0));
-    const int xo = (gb.lo[0] & 1) ? gb.lo[0] : gb.lo[0] - 1;
-    const int gx = (gb.hi[0] - xo + 1 + TTX - 1) / TTX, gy = (gb.len(1) + TTY - 1) / TTY;
-    // z chunks: minimise (waves of resident CTAs) x (planes per chunk + the 4
-    // warm-up/drain planes a chunk costs)
-    const int nzc = gb.len(2), ncols = gx * gy, slots = num_sms * tma_ctas_per_sm;
+  // z chunk of a TMA-fed sweep: minimise (waves of resident CTAs) x (planes
+  // per chunk + the 4 warm-up/drain planes a chunk costs)
+  int pick_zchunk(int nzc, int ncols, int slots) const {
     int best_nc = 1;
     double best = 1e300;
     for (int nc = 1; nc <= std::min(nzc, 64); nc++) {
@@ -526,11 +566,41 @@ class Engine : public EngineBase {
       const double cost = waves * (zc + 4);
       if (cost < best - 1e-9) { best = cost; best_nc = nc; }
     }
-    const int zc = zchunk_force > 0 ? std::min(zchunk_force, nzc) : (nzc + best_nc - 1) / best_nc;
+    return zchunk_force > 0 ? std::min(zchunk_force, nzc) : (nzc + best_nc - 1) / best_nc;
+  }
+  // row-warp sweep: tiles of RW_TX x RTY whose first column is odd
+  int fused_rw(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
+    if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
+    const Box gb = bbox(out, cube(g, 1, 0));
+    const int xo = (gb.lo[0] & 1) ? gb.lo[0] : gb.lo[0] - 1;
+    const int gx = (gb.hi[0] - xo + 1 + RW_TX - 1) / RW_TX, gy = (gb.len(1) + RTY - 1) / RTY;
+    const int nzc = gb.len(2), ncols = gx * gy;
+    const int zc = pick_zchunk(nzc, ncols, num_sms * rw_ctas_per_sm);
     const int nitems = ncols * ((nzc + zc - 1) / zc);
     if (nitems > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
     if (nblocks) *nblocks = nitems;
-    const dim3 grid(nitems), block((TTX / 2) * TTY);
+    const dim3 grid(nitems), block(rw_threads);
+    switch (rw_variant) {
+      case 1: return launch("hsmac_rw", k_hsmac_rw<8, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, (double*)P, D,
+                            out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+      case 2: return launch("hsmac_rw", k_hsmac_rw<5, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, (double*)P, D,
+                            out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+      default: return launch("hsmac_rw", k_hsmac_rw<13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, (double*)P,
+                             D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+    }
+  }
+  int fused_tma(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
+    if (use_rw) return fused_rw(set, D, out, fill_r, part, finalize, group_end, nblocks);
+    if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
+    const Box gb = bbox(out, cube(g, 1, 0));
+    const int xo = (gb.lo[0] & 1) ? gb.lo[0] : gb.lo[0] - 1;
+    const int gx = (gb.hi[0] - xo + 1 + TTX - 1) / TTX, gy = (gb.len(1) + TTY - 1) / TTY;
+    const int nzc = gb.len(2), ncols = gx * gy;
+    const int zc = pick_zchunk(nzc, ncols, num_sms * tma_ctas_per_sm);
+    const int nitems = ncols * ((nzc + zc - 1) / zc);
+    if (nitems > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
+    if (nblocks) *nblocks = nitems;
+    const dim3 grid(nitems), block(tma_threads);
     switch (tile_variant) {
       case 1: return launch("hsmac_tma", k_hsmac_tma<32, 16, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
                             (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);

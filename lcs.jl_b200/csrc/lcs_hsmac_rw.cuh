@@ -1,0 +1,443 @@
+// lcs_hsmac_rw.cuh -- the fused red-black HSMAC sweep, one warp per tile row.
+//
+// Same computation as k_hsmac_fused and k_hsmac_tma (both colour phases of
+// the reference's `foraxes(...; coloring=RedBlackFast())` sweep over a box D,
+// hsmac.jl:1-35, ping-ponged so that one pass replaces the two in-place
+// launches, bit-identical to them), arranged so that almost everything stays
+// in registers:
+//  - a CTA owns a tile of RW_TX x TY output cells of the x-y plane and streams
+//    along z through a chunk of planes; warp w owns the tile row y0-1+w
+//    (TY+3 rows: the rows of the tile, one below and two above);
+//  - lane l owns the x-pair (x0-2+2l, x0-1+2l), 16-byte aligned in HBM and in
+//    shared memory, so every shared-memory access is a 16-byte vector of a
+//    pair (or one 8-byte element of it);
+//  - in a row the colour-0 cell of every pair is on the same side at a given
+//    plane, so the colour logic is a compile-time branch per plane parity;
+//  - U, V, W, P of the previous plane and the pair's dp values stay in
+//    registers (indexed by plane parity, so nothing is moved between planes);
+//    x neighbours come from the adjacent lane (shuffles), y neighbours from
+//    shared memory (U, V, W and P planes loaded by TMA into a ring of 3 slots,
+//    and a ring of 3 dp planes);
+//  - planes away from the ends of a z chunk, and tiles away from the edges of
+//    D, run code without membership masks;
+//  - one __syncthreads per plane.
+//
+// Per plane s, in every warp (row j):
+//   phase X: dp0 of the colour-0 cell A at plane s, then dp1 of the same
+//            (i, j) at plane s-1, where A is colour 1; dp1 needs dp0 at s-1 of
+//            the x neighbours (registers of this and the adjacent lane), of
+//            the y neighbours (rows j-1, j+1 in shared memory) and dp0 at s
+//            (just computed) and s-2 (registers);
+//   barrier;
+//   phase Y: the faces U, V and P of plane s-1 and the faces W of plane s-2 of
+//            the pair, from old values in registers and dp of the pair (this
+//            lane), of x+1 (next lane) and of row j+1 (shared memory).
+// Waits on the mbarriers are bounded; a wait that runs out sets
+// ctx->wait_error and the kernel stops computing (the host reports
+// LCS_ETIMEDOUT).
+#pragma once
+
+#include <type_traits>
+
+#include "lcs_hsmac_tma.cuh"
+
+namespace lcs {
+namespace {
+
+constexpr int RW_TX = 60;  // output columns of a tile: pairs of lanes 1..30
+constexpr int RW_W = 64;   // columns of every shared-memory row: x0-2 .. x0+61
+
+template <int TY, int NS>
+struct RwLayout {
+  static constexpr int VH = TY + 4;  // velocity rows y0-2 .. y0+TY+1
+  static constexpr int DH = TY + 3;  // dp rows y0-1 .. y0+TY+1
+  static constexpr int NW = TY + 3;  // warps
+  static constexpr int NT = NW * 32;
+  static constexpr int VT = RW_W * VH;  // doubles of one field's plane tile
+  static constexpr int DP = RW_W * DH;  // doubles of one dp plane
+  static constexpr int PT = RW_W * TY;  // doubles of one P plane tile (rows y0 .. y0+TY-1)
+  static constexpr size_t vel_bytes = (size_t)NS * 3 * VT * 8;
+  static constexpr size_t p_bytes = (size_t)NS * PT * 8;
+  static constexpr size_t dp_bytes = (size_t)NS * DP * 8;
+  static constexpr size_t bar_bytes = 8 * NS;
+  static constexpr size_t red_bytes = 8 * 32;
+  static constexpr size_t total = vel_bytes + p_bytes + dp_bytes + bar_bytes + red_bytes + 16;
+  static_assert(NS == 3, "the dp ring shares the slot index of the TMA ring (3 planes)");
+  static_assert((VT * 8) % 128 == 0 && (PT * 8) % 128 == 0, "TMA destinations must stay 128-byte aligned");
+  static_assert((DP * 8) % 16 == 0, "dp rows must stay 16-byte aligned");
+  static_assert(NW <= 32, "one reduction slot per warp");
+};
+
+__device__ __forceinline__ double2 lds2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ double shfl_up1(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ double shfl_down1(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+// Per-lane (x) and per-warp (y) membership bits of one tile.
+struct RwBits {
+  // x, this lane's pair (L = x0-2+2l, R = L+1)
+  bool dLm, dL, dR, dRp;  // L-1, L, R, R+1 inside D
+  bool ownL, ownR;        // residual ownership
+  bool d1L, d1R;          // inside the dp1 region [x0, x0+RW_TX]
+  bool outL, outR;        // output column of this tile and inside `out`
+  bool intL, intR;        // interior column (P is stored on the interior only)
+  // y, this warp's row j
+  bool dym, dy, dyp;      // j-1, j, j+1 inside D
+  bool owny, d1y, outy, inty;
+  bool yrow;              // the row has outputs (rows y0 .. y0+TY-1)
+};
+
+
+// x0 (a tile's first output column) is odd: the pairs (x0-2+2l, x0-1+2l) and
+// the TMA box starting at x0-2 are then 16-byte aligned.  Work items are
+// (z chunk, tile column), chunk major, as in k_hsmac_tma.
+template <int TY, int NS>
+__global__ void __launch_bounds__(RwLayout<TY, NS>::NT, (RwLayout<TY, NS>::NT <= 256 ? 2 : 1))
+    k_hsmac_rw(Ctx* __restrict__ ctx, Grid g, int set, const __grid_constant__ TensorMaps tm,
+               double* __restrict__ P, Box D, Box out, Box gb, int x_origin, int gx, int gy, int zc, int nitems,
+               HsmacCoef cf, double* __restrict__ partials, int finalize, int group_end) {
+  using L = RwLayout<TY, NS>;
+  constexpr int NT = L::NT, VT = L::VT, DP = L::DP, W = RW_W;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int PT = L::PT;
+  double* svel = (double*)smem_raw;                               // [NS][3][VH][W]
+  double* sP = (double*)(smem_raw + L::vel_bytes);                // [NS][TY][W]
+  double* sdp = (double*)(smem_raw + L::vel_bytes + L::p_bytes);  // [NS][DH][W]
+  uint64_t* bars = (uint64_t*)(smem_raw + L::vel_bytes + L::p_bytes + L::dp_bytes);
+  double* red = (double*)(smem_raw + L::vel_bytes + L::p_bytes + L::dp_bytes + L::bar_bytes);
+  int* last_flag = (int*)(red + 32);
+
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const bool skip = ctx->cs.done != 0;
+  const int nx = g.n[0], ny = g.n[1], nz = g.n[2], h = g.h;
+  double racc = 0.0;
+
+  if (!skip) {
+    const int m0i = ctx->vphys[set][0], m1i = ctx->vphys[set][1], m2i = ctx->vphys[set][2];
+    double* Uo = (double*)ctx->vel[kSetSpare][0];
+    double* Vo = (double*)ctx->vel[kSetSpare][1];
+    double* Wo = (double*)ctx->vel[kSetSpare][2];
+    const double dxi = cf.dxi, dyi = cf.dyi, dzi = cf.dzi, dl = cf.dl, om = cf.omega;
+    const double dti = 1.0 / ctx->scal[0];
+    const int A = kAlignElems<double>;
+    const uint32_t plane_tx = (3u * VT + PT) * 8u;
+    if (tid == 0) {
+      for (int q = 0; q < NS; q++) mbar_init(&bars[q], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int ncols = gx * gy;
+    int loads = 0;  // plane loads issued by this CTA: slot = index % NS, parity = (index / NS) & 1
+    bool ok = true;
+    for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
+      const int col = item % ncols;
+      const int kb = gb.lo[2] + (item / ncols) * zc;
+      const int ke = min(gb.hi[2], kb + zc - 1);
+      const int x0 = x_origin + (col % gx) * RW_TX;
+      const int y0 = gb.lo[1] + (col / gx) * TY;
+      const int cx = x0 - 2 - 1 + A, cy = y0 - 2 + h - 1;
+      const int nplanes = ke - kb + 5;  // planes kb-2 .. ke+2
+      const int load0 = loads;
+      auto issue = [&](int l) {  // plane s = kb-2+l into slot (load0+l) % NS
+        const int li = load0 + l, slot = li % NS;
+        mbar_arrive_expect_tx(&bars[slot], plane_tx);
+        double* base = svel + slot * 3 * VT;
+        const int cz = kb - 2 + l + h - 1;
+        tma_load_3d(base, &tm.vel[m0i], &bars[slot], cx, cy, cz);
+        tma_load_3d(base + VT, &tm.vel[m1i], &bars[slot], cx, cy, cz);
+        tma_load_3d(base + 2 * VT, &tm.vel[m2i], &bars[slot], cx, cy, cz);
+        tma_load_3d(sP + slot * PT, &tm.P, &bars[slot], cx, cy + 2, cz);  // rows y0 .. y0+TY-1
+      };
+      if (tid == 0)
+        for (int l = 0; l < NS && l < nplanes; l++) issue(l);
+      loads += nplanes;
+
+      // ---- membership bits of this lane's pair and this warp's row ----------
+      const int xL = x0 - 2 + 2 * lane, xR = xL + 1, j = y0 - 1 + w;
+      const int ox_lo = max(x0, gb.lo[0]);
+      const int ox_hi = (x0 + RW_TX - 1 >= gb.hi[0]) ? gb.hi[0] + 1 : x0 + RW_TX - 1;
+      const int oy_hi = (y0 + TY - 1 >= gb.hi[1]) ? gb.hi[1] + 1 : y0 + TY - 1;
+      const int oz_hi = (ke >= gb.hi[2]) ? gb.hi[2] + 1 : ke;
+      auto inDx = [&](int i) { return i >= D.lo[0] && i <= D.hi[0]; };
+      auto inDy = [&](int y) { return y >= D.lo[1] && y <= D.hi[1]; };
+      auto ownx = [&](int i) { return i >= ox_lo && i <= ox_hi && i >= 1 && i <= nx + 1; };
+      auto outx = [&](int i) { return i >= x0 && i <= x0 + RW_TX - 1 && i >= out.lo[0] && i <= out.hi[0]; };
+      auto intx = [&](int i) { return i >= x0 && i <= x0 + RW_TX - 1 && i >= 1 && i <= nx; };
+      RwBits bt;
+      bt.dLm = inDx(xL - 1); bt.dL = inDx(xL); bt.dR = inDx(xR); bt.dRp = inDx(xR + 1);
+      bt.ownL = ownx(xL); bt.ownR = ownx(xR);
+      bt.d1L = xL >= x0 && xL <= x0 + RW_TX; bt.d1R = xR >= x0 && xR <= x0 + RW_TX;
+      bt.outL = outx(xL); bt.outR = outx(xR);
+      bt.intL = intx(xL); bt.intR = intx(xR);
+      bt.dym = inDy(j - 1); bt.dy = inDy(j); bt.dyp = inDy(j + 1);
+      bt.owny = j >= y0 && j <= oy_hi && j >= 1 && j <= ny + 1;
+      bt.d1y = j >= y0 && j <= y0 + TY;
+      bt.yrow = w >= 1 && w <= TY;
+      bt.outy = bt.yrow && j >= out.lo[1] && j <= out.hi[1];
+      bt.inty = bt.yrow && j >= 1 && j <= ny;
+      // Tiles whose every cell that matters lies inside D (x and y), whose
+      // outputs are interior and inside `out`, and which are not the last
+      // column (whose residual ownership reaches one cell further) need no x or
+      // y masks: their output and owned pairs are those of lanes 1..30.
+      const bool full = x0 - 1 >= D.lo[0] && x0 + RW_W - 3 <= D.hi[0] && y0 - 1 >= D.lo[1] &&
+                        y0 + TY + 1 <= D.hi[1] && x0 >= max(1, out.lo[0]) &&
+                        x0 + RW_TX - 1 <= min(nx, out.hi[0]) && y0 >= max(1, out.lo[1]) &&
+                        y0 + TY - 1 <= min(ny, out.hi[1]) && x0 + RW_TX - 1 < gb.hi[0];
+      // Planes s_lo .. s_hi need no z masks: every z condition below holds there.
+      const int s_lo = max(max(kb + 2, D.lo[2] + 2), max(out.lo[2] + 2, 2));
+      const int s_hi = min(min(min(ke + 1, D.hi[2]), min(oz_hi, nz + 1)), out.hi[2] + 1);
+      const int64_t grow = g.at(xL, j, 0);      // HBM offset of the pair at plane 0
+      const int vofs = (w + 1) * W + 2 * lane;  // this row's pair in a velocity plane tile
+      const int dofs = w * W + 2 * lane;        // this row's pair in a dp plane
+      const int pofs = (w - 1) * W + 2 * lane;  // this row's pair in a P plane tile (rows y0 ..)
+      const bool lane_out = lane >= 1 && lane <= 30;  // output pairs of a full tile
+
+      // Registers carried along z, indexed by plane parity q (q of plane s holds
+      // plane s): U, V (row j), V (row j-1), W and P of the plane; D0[q] = dp0 of
+      // the colour-0 cell of the pair at that plane; DM[q] = the final dp pair
+      // at s-1 computed at plane s; wb = W at s-2.
+      const double2 zero2 = make_double2(0.0, 0.0);
+      double2 Us2[2] = {zero2, zero2}, Vs2[2] = {zero2, zero2}, Vb2[2] = {zero2, zero2};
+      double2 Ws2[2] = {zero2, zero2}, Ps2[2] = {zero2, zero2}, DM[2] = {zero2, zero2};
+      double D0[2] = {0.0, 0.0};
+      double2 wb = zero2;
+      int sl = load0 % NS;  // ring slot of plane s (velocity, P and dp rings alike)
+      uint32_t par = (uint32_t)((load0 / NS) & 1);
+
+      // One plane: FULL (no x/y masks), ZF (no z masks), R (the colour-0 cell
+      // of the pair at s is the right one), Q (parity index of plane s).
+      auto plane = [&](int l, auto full_tag, auto zf_tag, auto r_tag, auto q_tag) -> bool {
+        constexpr bool FULL = decltype(full_tag)::value, ZF = decltype(zf_tag)::value;
+        constexpr bool R = decltype(r_tag)::value;
+        constexpr int Q = decltype(q_tag)::value, QM = 1 - Q;
+        const int s = kb - 2 + l;
+        if (!mbar_wait_bounded(&bars[sl], par)) {
+          ctx->wait_error = 1;
+          ok = false;
+        }
+        const bool do0 = ZF || s >= kb - 1, do1 = ZF || s - 1 >= kb;
+        const bool z_s = ZF || (s >= D.lo[2] && s <= D.hi[2]);
+        const bool z_m = ZF || (s - 1 >= D.lo[2] && s - 1 <= D.hi[2]);
+        const bool z_b = ZF || (s - 2 >= D.lo[2] && s - 2 <= D.hi[2]);
+        const bool own_s = ZF || (s >= kb && s <= oz_hi && s >= 1 && s <= nz + 1);
+        const bool own_m = ZF || (s - 1 >= kb && s - 1 <= oz_hi && s - 1 >= 1 && s - 1 <= nz + 1);
+        const int k1 = s - 1, k2 = s - 2;
+        const bool y1 = bt.yrow && (ZF || (k1 >= kb && k1 <= ke));  // U, V, P of plane s-1
+        const bool y2 = bt.yrow && (ZF || (k2 >= kb && k2 <= ke));  // W of plane s-2
+        const int slm = sl == 0 ? NS - 1 : sl - 1;
+        const double* Vt = svel + sl * 3 * VT;
+        Us2[Q] = lds2(Vt + vofs);
+        Vs2[Q] = lds2(Vt + VT + vofs);
+        Vb2[Q] = lds2(Vt + VT + vofs - W);
+        Ws2[Q] = lds2(Vt + 2 * VT + vofs);
+        if (bt.yrow) Ps2[Q] = lds2(sP + sl * PT + pofs);
+        const double2 us = Us2[Q], vs = Vs2[Q], vbs = Vb2[Q], ws = Ws2[Q];
+        const double2 um = Us2[QM], vm = Vs2[QM], vbm = Vb2[QM], wm = Ws2[QM];
+        const double d0p = D0[QM];   // dp0 at s-1 of the pair's colour-0 cell there
+        const double2 dpb = DM[QM];  // final dp pair at s-2
+        double* dps = sdp + sl * DP + dofs;   // this row's pair, plane s
+        double* dpm = sdp + slm * DP + dofs;  // this row's pair, plane s-1
+
+        // ---- phase X: dp0 at (A, s), dp1 at (A, s-1)
+        double d0 = 0.0, d1 = 0.0;
+        {
+          double upA = 0.0, upM = 0.0;  // U[xL-1] at s and s-1, from the lane below
+          if constexpr (!R) {
+            upA = shfl_up1(us.y);
+            upM = shfl_up1(um.y);
+          }
+          // dp0 at s-1 of the x neighbour held by the adjacent lane (A+1 for R, A-1 for L)
+          const double d0x = R ? shfl_down1(d0p) : shfl_up1(d0p);
+          const double uA = R ? us.y : us.x, uAm = R ? us.x : upA;
+          const double vA = R ? vs.y : vs.x, vbA = R ? vbs.y : vbs.x;
+          const double wA = R ? ws.y : ws.x, wmA = R ? wm.y : wm.x;
+          const bool inA = FULL || (bt.dy && (R ? bt.dR : bt.dL));
+          const bool m0 = do0 && z_s && inA;
+          const bool ownA = bt.owny && (FULL ? lane_out : (R ? bt.ownR : bt.ownL));
+          if (m0) {
+            const double dudx = dxi * (-uAm + uA);
+            const double dvdy = dyi * (-vbA + vA);
+            const double dwdz = dzi * (-wmA + wA);
+            const double div = dudx + dvdy + dwdz;
+            d0 = -om * div * dl;
+            if (own_s && ownA) racc += div * div;
+          }
+          if (do0) dps[R ? 1 : 0] = d0;
+          const bool m1 = do1 && z_m && bt.d1y && inA;
+          if (m1) {
+            const double dyl = dpm[(R ? 1 : 0) - W], dyu = dpm[(R ? 1 : 0) + W];  // dp0 of rows j-1, j+1
+            double ul = R ? um.x : upM, ur = R ? um.y : um.x;
+            double vl = R ? vbm.y : vbm.x, vr = R ? vm.y : vm.x;
+            double wl = R ? wb.y : wb.x, wr = R ? wm.y : wm.x;
+            const double cl = (R ? d0p : d0x) * dxi, cr = (R ? d0x : d0p) * dxi;
+            const double cd = dyl * dyi, cu = dyu * dyi;
+            const double cb = (R ? dpb.y : dpb.x) * dzi, ct = d0 * dzi;
+            ul = (FULL || (R ? bt.dL : bt.dLm)) ? ul + cl : ul;
+            ur = (FULL || (R ? bt.dRp : bt.dR)) ? ur - cr : ur;
+            vl = (FULL || bt.dym) ? vl + cd : vl;
+            vr = (FULL || bt.dyp) ? vr - cu : vr;
+            wl = z_b ? wl + cb : wl;
+            wr = m0 ? wr - ct : wr;
+            const double dudx = dxi * (-ul + ur);
+            const double dvdy = dyi * (-vl + vr);
+            const double dwdz = dzi * (-wl + wr);
+            const double div = dudx + dvdy + dwdz;
+            d1 = -om * div * dl;
+            if (own_m && ownA) racc += div * div;
+          }
+          if (do1 && bt.d1y && (FULL || (R ? bt.d1R : bt.d1L))) dpm[R ? 1 : 0] = d1;
+        }
+        D0[Q] = d0;
+        const double2 dm = R ? make_double2(d0p, d1) : make_double2(d1, d0p);  // final dp at s-1
+        DM[Q] = dm;
+        if (__syncthreads_or(!ok)) return false;
+        if (tid == 0 && l + NS < nplanes) issue(l + NS);  // every warp is past its reads of this slot
+
+        // ---- phase Y: U, V, P at s-1 and W at s-2 of the pair
+        const double dN = shfl_down1(dm.x);  // dp(xR+1, s-1)
+        const double2 pv = Ps2[QM];          // P at s-1
+        const int64_t o1 = grow + (int64_t)k1 * g.pz;
+        if (y1) {
+          const double2 dup = lds2(dpm + W);  // final dp of row j+1 at s-1
+          const bool mL = z_m && (FULL || (bt.dy && bt.dL)), mR = z_m && (FULL || (bt.dy && bt.dR));
+          const bool mRp = z_m && (FULL || (bt.dy && bt.dRp));
+          const bool upL = z_m && (FULL || (bt.dyp && bt.dL)), upR = z_m && (FULL || (bt.dyp && bt.dR));
+          // the left cell is colour 0 at s-1 exactly when R
+          const double u0 = face_update(um.x, R, mL, dm.x, mR, dm.y, dxi);
+          const double u1 = face_update(um.y, !R, mR, dm.y, mRp, dN, dxi);
+          const double v0 = face_update(vm.x, R, mL, dm.x, upL, dup.x, dyi);
+          const double v1 = face_update(vm.y, !R, mR, dm.y, upR, dup.y, dyi);
+          const double p0 = mL ? pv.x + dm.x * dti : pv.x;
+          const double p1 = mR ? pv.y + dm.y * dti : pv.y;
+          if (FULL) {
+            if (lane_out) {
+              *reinterpret_cast<double2*>(Uo + o1) = make_double2(u0, u1);
+              *reinterpret_cast<double2*>(Vo + o1) = make_double2(v0, v1);
+              *reinterpret_cast<double2*>(P + o1) = make_double2(p0, p1);  // interior: 1 <= k1 <= nz in ZF
+            }
+          } else {
+            const bool oy = bt.outy && k1 >= out.lo[2] && k1 <= out.hi[2];
+            const bool oL = oy && bt.outL, oR = oy && bt.outR;
+            if (oL && oR) {
+              *reinterpret_cast<double2*>(Uo + o1) = make_double2(u0, u1);
+              *reinterpret_cast<double2*>(Vo + o1) = make_double2(v0, v1);
+            } else {
+              if (oL) { Uo[o1] = u0; Vo[o1] = v0; }
+              if (oR) { Uo[o1 + 1] = u1; Vo[o1 + 1] = v1; }
+            }
+            // P in place on the interior only (P halos are refilled before any read)
+            const bool pj = bt.inty && k1 >= 1 && k1 <= nz;
+            const bool pL = pj && bt.intL, pR = pj && bt.intR;
+            if (pL && pR) {
+              *reinterpret_cast<double2*>(P + o1) = make_double2(p0, p1);
+            } else {
+              if (pL) P[o1] = p0;
+              if (pR) P[o1 + 1] = p1;
+            }
+          }
+        }
+        if (y2) {
+          // W faces between planes s-2 and s-1; the left cell is colour 0 at s-2 exactly when !R
+          const bool mxL = FULL || (bt.dy && bt.dL), mxR = FULL || (bt.dy && bt.dR);
+          const double w0 = face_update(wb.x, !R, z_b && mxL, dpb.x, z_m && mxL, dm.x, dzi);
+          const double w1 = face_update(wb.y, R, z_b && mxR, dpb.y, z_m && mxR, dm.y, dzi);
+          const int64_t o2 = o1 - g.pz;
+          if (FULL) {
+            if (lane_out) *reinterpret_cast<double2*>(Wo + o2) = make_double2(w0, w1);
+          } else {
+            const bool oy = bt.outy && k2 >= out.lo[2] && k2 <= out.hi[2];
+            const bool oL = oy && bt.outL, oR = oy && bt.outR;
+            if (oL && oR) {
+              *reinterpret_cast<double2*>(Wo + o2) = make_double2(w0, w1);
+            } else {
+              if (oL) Wo[o2] = w0;
+              if (oR) Wo[o2 + 1] = w1;
+            }
+          }
+        }
+        wb = wm;
+        if (++sl == NS) {
+          sl = 0;
+          par ^= 1u;
+        }
+        return true;
+      };
+
+      using T_ = std::true_type;
+      using F_ = std::false_type;
+      using Q0 = std::integral_constant<int, 0>;
+      using Q1 = std::integral_constant<int, 1>;
+      auto run = [&](auto full_tag) {
+        int l = 0;
+        while (l < nplanes) {
+          const int s = kb - 2 + l;
+          const bool ar = ((j + s) & 1) == 0;  // the colour-0 cell at s is the right one
+          bool good;
+          if ((l & 1) == 0 && s >= s_lo && s + 1 <= s_hi) {
+            // two planes without z masks (the colour-0 side flips between them)
+            if (ar) {
+              good = plane(l, full_tag, T_{}, T_{}, Q0{}) && plane(l + 1, full_tag, T_{}, F_{}, Q1{});
+            } else {
+              good = plane(l, full_tag, T_{}, F_{}, Q0{}) && plane(l + 1, full_tag, T_{}, T_{}, Q1{});
+            }
+            l += 2;
+          } else {
+            if (l & 1) {
+              good = ar ? plane(l, F_{}, F_{}, T_{}, Q1{}) : plane(l, F_{}, F_{}, F_{}, Q1{});
+            } else {
+              good = ar ? plane(l, F_{}, F_{}, T_{}, Q0{}) : plane(l, F_{}, F_{}, F_{}, Q0{});
+            }
+            l += 1;
+          }
+          if (!good) {
+            ok = false;
+            break;
+          }
+        }
+      };
+      if (full) {
+        run(T_{});
+      } else {
+        run(F_{});
+      }
+    }
+    if (!ok) {
+      // let the copies already issued land before the CTA's shared memory goes away
+      if (tid == 0)
+        for (int q = 0; q < NS; q++) mbar_wait_bounded(&bars[q], 0u);
+      __syncthreads();
+    }
+  }
+  // residual partial of this CTA; the last CTA finalizes the sweep and swaps
+  const double bs = block_sum<NT>(racc, red);
+  const unsigned int nb = gridDim.x;
+  const unsigned int bid = blockIdx.x;
+  if (tid == 0) partials[bid] = bs;
+  if (last_block(&ctx->ticket, nb, last_flag)) {
+    if (skip || ctx->wait_error) {
+      if (tid == 0) {
+        ctx->ticket = 0;
+        if (ctx->wait_error) ctx->cs.done = 1;
+      }
+      return;
+    }
+    if (finalize) {
+      double v = 0.0;
+      for (int q = tid; q < (int)nb; q += NT) v += __ldcg(&partials[q]);
+      const double s2 = block_sum<NT>(v, red);
+      if (tid == 0) hsmac_check(ctx, cf, s2, group_end);
+    }
+    if (tid == 0) {
+      ctx->ticket = 0;
+      for (int c = 0; c < 3; c++) {
+        void* tmp = ctx->vel[set][c];
+        ctx->vel[set][c] = ctx->vel[kSetSpare][c];
+        ctx->vel[kSetSpare][c] = tmp;
+        const int tp = ctx->vphys[set][c];
+        ctx->vphys[set][c] = ctx->vphys[kSetSpare][c];
+        ctx->vphys[kSetSpare][c] = tp;
+      }
+    }
+  }
+}
+}  // namespace
+}  // namespace lcs

@@ -85,6 +85,16 @@ struct TmaLayout {
   static_assert((P_TILE * 8) % 128 == 0, "TMA destinations must stay 128-byte aligned");
 };
 
+// Threads of a CTA: one per phase-X item (an x-pair of the dp region, whose
+// rows are y0-1 .. y0+TY+1), rounded up to whole warps; the first
+// (TX/2)*TY of them also own an output pair in phase Y.
+template <int TX, int TY>
+struct TmaThreads {
+  static constexpr int NITEM = (TX / 2 + 2) * (TY + 3);
+  static constexpr int NT = (NITEM + 31) / 32 * 32;
+  static constexpr int MINB = NT <= 512 ? 2 : 1;  // resident CTAs the register budget is sized for
+};
+
 // Adds the contributions of the two cells sharing a face in the order of the
 // in-place sweep: the colour-0 cell's first, then the colour-1 cell's.
 // `sa` is +1 for the face's lower cell (its own face, `+= dp*dci`) and the
@@ -119,7 +129,7 @@ __device__ __forceinline__ double face_update(double val, bool lower_first, bool
 //   phase Y: faces U, V and P at plane s-1, faces W at plane s-2 (which need
 //            dp at s-2 and s-1, both complete after phase X).
 template <int TX, int TY, int NS>
-__global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ ctx, Grid g, int set,
+__global__ void __launch_bounds__(TmaThreads<TX, TY>::NT, TmaThreads<TX, TY>::MINB) k_hsmac_tma(Ctx* __restrict__ ctx, Grid g, int set,
                                                             const __grid_constant__ TensorMaps tm,
                                                             double* __restrict__ P, Box D, Box out, Box gb,
                                                             int x_origin, int gx, int gy, int zc, int nitems,
@@ -127,7 +137,8 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
                                                             double* __restrict__ partials, int finalize,
                                                             int group_end) {
   using L = TmaLayout<TX, TY, NS>;
-  constexpr int NT = (TX / 2) * TY;
+  constexpr int NT = TmaThreads<TX, TY>::NT;
+  constexpr int NP = (TX / 2) * TY;  // output pairs (phase Y)
   constexpr int PW = TX / 2 + 2;                  // pairs per row of the dp region (x0-1 .. x0+TX+2)
   constexpr int NITEM = PW * (TY + 3);            // rows y0-1 .. y0+TY+1
   constexpr int NROUND = (NITEM + NT - 1) / NT;
@@ -222,7 +233,8 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
         for (int o = 0; o <= 1; o++) b |= ((2 * pp + o <= TX + 2) ? 1u : 0u) << (13 + o);
         it_bits[rd] = b;
       }
-      // output pair of phase Y: cells (x0+2op, x0+2op+1) in row y0+orow
+      // output pair of phase Y (threads tid < NP): cells (x0+2op, x0+2op+1) in row y0+orow
+      const bool ythread = tid < NP;
       const int op = tid % (TX / 2), orow = tid / (TX / 2);
       const int oi = x0 + 2 * op, oj = y0 + orow;
       // bits 0..2: x in D of oi..oi+2; 3, 4: y in D of oj, oj+1; 5, 6: x in out;
@@ -329,7 +341,7 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
         // ---- phase Y: U, V, P at k1 = s-1; W at k2 = s-2
         const int k1 = s - 1, k2 = s - 2;
         const bool lower_first1 = ((oij + k1) & 1) == 0;  // cell oi is colour 0 at k1
-        if (k1 >= kb && k1 <= ke) {
+        if (ythread && k1 >= kb && k1 <= ke) {
           const double dA = d_m[o_dofs], dB = d_m[o_dofs + 1], dC = d_m[o_dofs + 2];
           const bool mA = z_m && (FULL || (((ob >> 0) & 1u) && ((ob >> 3) & 1u)));
           const bool mB = z_m && (FULL || (((ob >> 1) & 1u) && ((ob >> 3) & 1u)));
@@ -365,7 +377,7 @@ __global__ void __launch_bounds__((TX / 2) * TY) k_hsmac_tma(Ctx* __restrict__ c
             if (pb) P[o + 1] = p1;
           }
         }
-        if (k2 >= kb && k2 <= ke) {
+        if (ythread && k2 >= kb && k2 <= ke) {
           // W face between planes k2 and k1 = k2+1; cell oi at k2 has colour 1-c0(k1)
           const bool mxA = FULL || (((ob >> 0) & 1u) && ((ob >> 3) & 1u));
           const bool mxB = FULL || (((ob >> 1) & 1u) && ((ob >> 3) & 1u));

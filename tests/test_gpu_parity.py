@@ -64,10 +64,11 @@ def test_update_and_fused_rhs_update_bitwise(stage):
 VARIANTS = [(tb, ov) for tb in (True, False) for ov in (True, False)]
 
 
-@pytest.fixture(params=["tma", "plain"])
+@pytest.fixture(params=["rw", "tma", "plain"])
 def sweep(request, monkeypatch):
-    """Both implementations of the fused red-black sweep: the TMA-fed one
-    (default for red-black-fast) and the plain-load one."""
+    """The implementations of the fused red-black sweep: the row-warp one
+    (default for red-black-fast), the thread-per-item TMA one and the
+    plain-load one."""
     monkeypatch.setenv("LCS_B200_FUSED_SWEEP", request.param)
     return request.param
 
@@ -112,17 +113,40 @@ def test_hsmac_long_runs_and_early_exit(tb, ov, n, epsp, sweep):
 
 
 @pytest.mark.parametrize("tb,ov", VARIANTS)
-def test_tma_sweep_equals_plain_sweep_128(tb, ov, monkeypatch):
-    """At 128^3 (several tiles and z chunks per sweep) the TMA-fed and the
-    plain-load fused sweeps give identical fields."""
+def test_tma_sweeps_equal_plain_sweep_128(tb, ov, monkeypatch):
+    """At 128^3 (several tiles and z chunks per sweep) the two TMA-fed sweeps
+    and the plain-load sweep give identical fields."""
     from lcs_b200 import inits
 
     out = []
-    for mode in ("tma", "plain"):
+    for mode in ("rw", "tma", "plain"):
         monkeypatch.setenv("LCS_B200_FUSED_SWEEP", mode)
         e = Engine(make_config(128, mode=F.MODE_FLOW, time_blocking=tb, overlap=ov, itrmin=6, itrmax=12,
                                epsp=1e-12))
         U, V, W, P = inits.spectral_flow(128, seed=4)
+        e.upload_flow(U, V, W, P)
+        lg = e.couple(2, 0.003)
+        out.append((lg, e.download_flow()))
+        e.close()
+    lb, fb = out[-1]
+    for la, fa in out[:-1]:
+        assert la["itr"] == lb["itr"] and abs(la["div"] - lb["div"]) <= 1e-13 * lb["div"]
+        for a, b in zip(fa, fb):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("variant", ["8", "5"])
+def test_row_warp_variants_equal_default(variant, monkeypatch):
+    """The row-warp sweep's other tile heights and ring depths give the same
+    fields as the default one (96^3: partial tiles in x and y)."""
+    from lcs_b200 import inits
+
+    out = []
+    for v in (variant, "13"):
+        monkeypatch.setenv("LCS_B200_RW", v)
+        e = Engine(make_config(96, mode=F.MODE_FLOW, time_blocking=True, overlap=True, itrmin=6, itrmax=9,
+                               epsp=1e-12))
+        U, V, W, P = inits.spectral_flow(96, seed=11)
         e.upload_flow(U, V, W, P)
         lg = e.couple(2, 0.003)
         out.append((lg, e.download_flow()))

@@ -56,10 +56,13 @@ WORKLOADS = {
                   precision="fp64"),
 }
 
-# DRAM bytes (read + write) per launch of the sweep kernel, per interior cell,
-# from one `ncu --set full` capture of `python bench.py --steps 1 --warmup 0
-# --no-cpu-baseline` (rc256); filled in per kernel once it has been captured.
-SWEEP_DRAM_BYTES_PER_CELL = {}
+# DRAM bytes (read + write) per launch of the sweep kernel, per interior cell:
+# dram__bytes_read.sum + dram__bytes_write.sum of two launches captured by
+# `ncu --set full --clock-control none -k regex:hsmac_rw -s 50 -c 2` on
+# `python bench.py --steps 1 --warmup 0 --no-cpu-baseline` (rc256), averaged:
+# 1135.9 MB and 1200.2 MB per launch over 256^3 cells.
+SWEEP_DRAM_BYTES_PER_CELL = {"hsmac_rw": 69.6}
+SWEEP_KERNELS = ("hsmac_rw", "hsmac_tma", "hsmac_fused")
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
@@ -221,7 +224,8 @@ def cpu_baseline(rc, w, budget_s=30.0):
 
 
 def run_reference(args):
-    world, rank, local = dist_setup()
+    """Rank 0 alone times the CPU restatement; other ranks exit without work."""
+    rank = int(os.environ.get("RANK", "0"))
     rc, w = make_run_config(args.workload)
     line = None
     if rank == 0:
@@ -238,7 +242,6 @@ def run_reference(args):
                         "d2h_bytes_per_step": 0},
                 "particle_steps_per_s": base["particle_steps_per_s"]}
         print(json.dumps(line), flush=True)
-    barrier(world)
     return 0
 
 
@@ -277,7 +280,7 @@ def run_b200(args):
     # the graph replays the same kernels with the same loop counts
     launches = int(round(sum(v[1] for v in tot.values()) / prof_steps * args.steps))
     # the dominant kernel: the fused red-black sweep (TMA-fed, or the plain form)
-    sweep_kernel = max(("hsmac_tma", "hsmac_fused"), key=lambda k: tot.get(k, (0.0, 0))[0])
+    sweep_kernel = max(SWEEP_KERNELS, key=lambda k: tot.get(k, (0.0, 0))[0])
     ms_sweep, cnt = tot.get(sweep_kernel, (0.0, 0))
     T = 8
     peak, peak_kind = hbm_peak()

@@ -14,6 +14,8 @@
 namespace lcs {
 EngineBase* make_engine_f64(const lcs_config& c, std::string* err, int* rc);
 int64_t footprint_f64(const lcs_config& c);
+EngineBase* make_engine_f32(const lcs_config& c, std::string* err, int* rc);
+int64_t footprint_f32(const lcs_config& c);
 }  // namespace lcs
 
 struct lcs_handle {
@@ -75,7 +77,6 @@ static int validate(const lcs_config* c, std::string* why) {
     if (!(c->species[s].density_ratio > 0)) { *why = "density_ratio must be positive"; return LCS_EINVAL; }
   }
   if (c->precision != LCS_PRECISION_FP64 && c->precision != LCS_PRECISION_FP32_MIXED) { *why = "bad precision"; return LCS_EINVAL; }
-  if (c->precision == LCS_PRECISION_FP32_MIXED) { *why = "the FP32-mixed form is not built into this library yet"; return LCS_EINVAL; }
   return LCS_OK;
 }
 
@@ -86,7 +87,7 @@ int lcs_footprint(const lcs_config* cfg, int64_t* bytes) {
   int rc = validate(cfg, &why);
   if (rc) return set_global_error(rc, why.c_str());
   if (!bytes) return set_global_error(LCS_EINVAL, "null output");
-  *bytes = lcs::footprint_f64(*cfg);
+  *bytes = cfg->precision == LCS_PRECISION_FP32_MIXED ? lcs::footprint_f32(*cfg) : lcs::footprint_f64(*cfg);
   return LCS_OK;
 }
 
@@ -103,7 +104,8 @@ int lcs_create(const lcs_config* cfg, lcs_handle** out) {
     return set_global_error(LCS_ECUDA, "no CUDA device available for the B200 backend");
   }
   if (cfg->device < 0 || cfg->device >= ndev) return set_global_error(LCS_EINVAL, "device ordinal out of range");
-  lcs::EngineBase* eng = lcs::make_engine_f64(*cfg, &why, &rc);
+  lcs::EngineBase* eng = cfg->precision == LCS_PRECISION_FP32_MIXED ? lcs::make_engine_f32(*cfg, &why, &rc)
+                                                                     : lcs::make_engine_f64(*cfg, &why, &rc);
   if (!eng) return set_global_error(rc, why.c_str());
   lcs_handle* h = new (std::nothrow) lcs_handle;
   if (!h) {

@@ -257,11 +257,12 @@ class Engine : public EngineBase {
     if (c.forcing == LCS_FORCING_RC_ENERGY) LCS_TRY(init_rcf());
     // the TMA-fed sweeps serve red-black-fast (the production colouring): the
     // row-warp kernel by default; LCS_B200_FUSED_SWEEP=tma selects the
-    // thread-per-item TMA kernel, =plain the plain-load sweep
+    // thread-per-item TMA kernel (FP64 only), =plain the plain-load sweep
     const char* sweep = std::getenv("LCS_B200_FUSED_SWEEP");
     const std::string sw = sweep ? std::string(sweep) : std::string("rw");
-    use_tma = std::is_same<T, double>::value && c.coloring == LCS_COLORING_RED_BLACK_FAST && sw != "plain";
-    use_rw = use_tma && sw != "tma";
+    constexpr bool f64 = std::is_same<T, double>::value;
+    use_tma = c.coloring == LCS_COLORING_RED_BLACK_FAST && sw != "plain";
+    use_rw = use_tma && !(f64 && sw == "tma");
     if (use_tma) LCS_TRY(init_tma());
     LCS_TRY(init_faces());
     LCS_CUDA(cudaStreamSynchronize(stream));
@@ -283,7 +284,7 @@ class Engine : public EngineBase {
       tile_variant = v == "32x16" ? 1 : v == "32x8" ? 2 : v == "64x16" ? 3 : 0;
     }
     if (const char* z = std::getenv("LCS_B200_ZCHUNK")) zchunk_force = std::atoi(z);
-    switch (tile_variant) {
+    if (std::is_same<T, double>::value) switch (tile_variant) {
       case 1: TTX = 32; TTY = 16; tma_smem = TmaLayout<32, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 16, TNS>;
               tma_threads = TmaThreads<32, 16>::NT; break;
       case 2: TTX = 32; TTY = 8; tma_smem = TmaLayout<32, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 8, TNS>;
@@ -298,54 +299,60 @@ class Engine : public EngineBase {
     LCS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
     if (!fn || q != cudaDriverEntryPointSuccess) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled is unavailable");
     auto encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    const CUtensorMapDataType dtype =
+        std::is_same<T, double>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)(g.n[1] + 2 * g.h), (cuuint64_t)(g.n[2] + 2 * g.h)};
     const cuuint64_t strides[2] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.pz * sizeof(T)};
     const cuuint32_t estr[3] = {1, 1, 1};
     const cuuint32_t vbox[3] = {(cuuint32_t)TTX + 4, (cuuint32_t)TTY + 4, 1};
     const cuuint32_t pbox[3] = {(cuuint32_t)TTX, (cuuint32_t)TTY, 1};
-    for (int b = 0; b < kVelMaps; b++) {
-      CUresult r = encode(&tmaps.vel[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, vel0[b / 3][b % 3], dims, strides, vbox,
-                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (velocity %d) failed: %d", b, (int)r);
+    if (std::is_same<T, double>::value && !use_rw) {  // the thread-per-item kernel (FP64)
+      for (int b = 0; b < kVelMaps; b++) {
+        CUresult r = encode(&tmaps.vel[b], dtype, 3, vel0[b / 3][b % 3], dims, strides, vbox, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (velocity %d) failed: %d", b, (int)r);
+      }
+      CUresult r = encode(&tmaps.P, dtype, 3, (void*)P, dims, strides, pbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (P) failed: %d", (int)r);
+      LCS_CUDA(cudaFuncSetAttribute(tma_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem));
+      LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_ctas_per_sm, tma_fn, tma_threads, tma_smem));
+      if (tma_ctas_per_sm < 1) return fail(LCS_ECUDA, "the TMA sweep does not fit on an SM");
     }
-    CUresult r = encode(&tmaps.P, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)P, dims, strides, pbox, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (P) failed: %d", (int)r);
+    LCS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, cfg.device));
     if (use_rw) {
-      // row-warp sweep: LCS_B200_RW=13 (tile rows, default) | 8 | 5
+      // row-warp sweep tile rows: LCS_B200_RW=13 (default: one CTA of 16 warps
+      // per SM, fastest in both precisions) | 8 | 5
+      rw_variant = 0;
       if (const char* v = std::getenv("LCS_B200_RW")) {
         const std::string t(v);
         rw_variant = t == "8" ? 1 : t == "5" ? 2 : 0;
       }
       switch (rw_variant) {
-        case 1: RTY = 8; rw_smem = RwLayout<8, 3>::total; rw_fn = (const void*)k_hsmac_rw<8, 3>;
-                rw_threads = RwLayout<8, 3>::NT; break;
-        case 2: RTY = 5; rw_smem = RwLayout<5, 3>::total; rw_fn = (const void*)k_hsmac_rw<5, 3>;
-                rw_threads = RwLayout<5, 3>::NT; break;
-        default: RTY = 13; rw_smem = RwLayout<13, 3>::total; rw_fn = (const void*)k_hsmac_rw<13, 3>;
-                 rw_threads = RwLayout<13, 3>::NT; break;
+        case 1: RTY = 8; rw_smem = RwLayout<T, 8, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 8, 3>;
+                rw_threads = RwLayout<T, 8, 3>::NT; break;
+        case 2: RTY = 5; rw_smem = RwLayout<T, 5, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 5, 3>;
+                rw_threads = RwLayout<T, 5, 3>::NT; break;
+        default: RTY = 13; rw_smem = RwLayout<T, 13, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 13, 3>;
+                 rw_threads = RwLayout<T, 13, 3>::NT; break;
       }
       const cuuint32_t rbox[3] = {(cuuint32_t)RW_W, (cuuint32_t)RTY + 4, 1};
       for (int b = 0; b < kVelMaps; b++) {
-        CUresult rr = encode(&tmaps_rw.vel[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, vel0[b / 3][b % 3], dims, strides,
+        CUresult rr = encode(&tmaps_rw.vel[b], dtype, 3, vel0[b / 3][b % 3], dims, strides,
                              rbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (rr != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp velocity %d) failed: %d", b,
                                             (int)rr);
       }
       const cuuint32_t rpbox[3] = {(cuuint32_t)RW_W, (cuuint32_t)RTY, 1};
-      CUresult rp = encode(&tmaps_rw.P, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)P, dims, strides, rpbox, estr,
+      CUresult rp = encode(&tmaps_rw.P, dtype, 3, (void*)P, dims, strides, rpbox, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       if (rp != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp P) failed: %d", (int)rp);
       LCS_CUDA(cudaFuncSetAttribute(rw_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
     }
-    LCS_CUDA(cudaFuncSetAttribute(tma_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem));
-    LCS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, cfg.device));
-    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_ctas_per_sm, tma_fn, tma_threads, tma_smem));
-    if (tma_ctas_per_sm < 1) return fail(LCS_ECUDA, "the TMA sweep does not fit on an SM");
     if (use_rw) {
       LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rw_ctas_per_sm, rw_fn, rw_threads, rw_smem));
       if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the row-warp sweep does not fit on an SM");
@@ -506,7 +513,8 @@ class Engine : public EngineBase {
       for (int q = 0; q < 3; q++) { fa.set[fa.nf] = set; fa.comp[fa.nf] = q; fa.ptr[fa.nf] = nullptr; fa.nf++; }
     if (withP) { fa.set[fa.nf] = -1; fa.comp[fa.nf] = 0; fa.ptr[fa.nf] = P; fa.nf++; }
     const int64_t total = fill_count(g, r, full);
-    return launch("synchalo", k_fill_halo<T>, dim3(blocks_for(total, 256)), dim3(256), 0, (const Ctx*)dctx, g, fa, r,
+    if (total >= INT32_MAX) return fail(LCS_EINVAL, "halo too large for 32-bit fill indices");
+    return launch("synchalo", k_fill_halo<T>, dim3(blocks_for(total, 256, 148 * 32)), dim3(256), 0, (const Ctx*)dctx, g, fa, r,
                   full, total);
   }
 
@@ -572,7 +580,11 @@ class Engine : public EngineBase {
   int fused_rw(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
     if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
     const Box gb = bbox(out, cube(g, 1, 0));
-    const int xo = (gb.lo[0] & 1) ? gb.lo[0] : gb.lo[0] - 1;
+    // first tile column: the largest x0 <= gb.lo[0] with x0-2 on a 16-byte
+    // boundary (x0 odd in FP64, x0 = 3 mod 4 in FP32); tiles step by RW_TX = 60
+    const int am = 16 / (int)sizeof(T), ar = am - 1;
+    int xo = gb.lo[0];
+    while (((xo % am) + am) % am != ar % am) xo--;
     const int gx = (gb.hi[0] - xo + 1 + RW_TX - 1) / RW_TX, gy = (gb.len(1) + RTY - 1) / RTY;
     const int nzc = gb.len(2), ncols = gx * gy;
     const int zc = pick_zchunk(nzc, ncols, num_sms * rw_ctas_per_sm);
@@ -581,16 +593,17 @@ class Engine : public EngineBase {
     if (nblocks) *nblocks = nitems;
     const dim3 grid(nitems), block(rw_threads);
     switch (rw_variant) {
-      case 1: return launch("hsmac_rw", k_hsmac_rw<8, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, (double*)P, D,
+      case 1: return launch("hsmac_rw", k_hsmac_rw<T, 8, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P, D,
                             out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
-      case 2: return launch("hsmac_rw", k_hsmac_rw<5, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, (double*)P, D,
+      case 2: return launch("hsmac_rw", k_hsmac_rw<T, 5, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P, D,
                             out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
-      default: return launch("hsmac_rw", k_hsmac_rw<13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, (double*)P,
+      default: return launch("hsmac_rw", k_hsmac_rw<T, 13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P,
                              D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
     }
   }
   int fused_tma(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
     if (use_rw) return fused_rw(set, D, out, fill_r, part, finalize, group_end, nblocks);
+    if (!std::is_same<T, double>::value) return fail(LCS_EINVAL, "the thread-per-item TMA sweep is FP64 only");
     if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
     const Box gb = bbox(out, cube(g, 1, 0));
     const int xo = (gb.lo[0] & 1) ? gb.lo[0] : gb.lo[0] - 1;
@@ -666,8 +679,11 @@ class Engine : public EngineBase {
     Box f[6];
     faces_of(dom, core, f);
     const bool core_nonempty = core.len(0) > 0 && core.len(1) > 0 && core.len(2) > 0;
+    int64_t slab_cells = 0;  // the face kernel indexes a pair of slabs with 32-bit integers
+    for (int q = 0; q < 6; q++)
+      slab_cells = std::max<int64_t>(slab_cells, (int64_t)((f[q].len(0) + 1) / 2) * f[q].len(1) * f[q].len(2));
     if (face_grid > 0 && core_nonempty && cfg.coloring != LCS_COLORING_RED_BLACK_BLOCK &&
-        used + face_grid <= plan.partials_cap) {
+        used + face_grid <= plan.partials_cap && 2 * slab_cells < INT32_MAX) {
       FaceSet fs;
       for (int q = 0; q < 6; q++) fs.f[q] = f[q];
       return launch_coop("hsmac_faces", k_hsmac_faces<T>, dim3(face_grid), dim3(256), dctx, g, set, P, fs, hc,

@@ -8,9 +8,9 @@
 //  - a CTA owns a tile of RW_TX x TY output cells of the x-y plane and streams
 //    along z through a chunk of planes; warp w owns the tile row y0-1+w
 //    (TY+3 rows: the rows of the tile, one below and two above);
-//  - lane l owns the x-pair (x0-2+2l, x0-1+2l), 16-byte aligned in HBM and in
-//    shared memory, so every shared-memory access is a 16-byte vector of a
-//    pair (or one 8-byte element of it);
+//  - lane l owns the x-pair (x0-2+2l, x0-1+2l), aligned to the pair's size in
+//    HBM and in shared memory, so every shared-memory access is a vector of a
+//    pair (or one element of it);
 //  - in a row the colour-0 cell of every pair is on the same side at a given
 //    plane, so the colour logic is a compile-time branch per plane parity;
 //  - U, V, W, P of the previous plane and the pair's dp values stay in
@@ -47,30 +47,60 @@ namespace {
 constexpr int RW_TX = 60;  // output columns of a tile: pairs of lanes 1..30
 constexpr int RW_W = 64;   // columns of every shared-memory row: x0-2 .. x0+61
 
-template <int TY, int NS>
+// Pair vector of the field type (a lane's two cells).
+template <typename T> struct Pair2;
+template <> struct Pair2<double> { using type = double2; };
+template <> struct Pair2<float> { using type = float2; };
+template <typename T> using pair_t = typename Pair2<T>::type;
+template <typename T> __device__ __forceinline__ pair_t<T> mk2(T a, T b) { return pair_t<T>{a, b}; }
+
+template <typename T, int TY, int NS>
 struct RwLayout {
   static constexpr int VH = TY + 4;  // velocity rows y0-2 .. y0+TY+1
   static constexpr int DH = TY + 3;  // dp rows y0-1 .. y0+TY+1
   static constexpr int NW = TY + 3;  // warps
   static constexpr int NT = NW * 32;
-  static constexpr int VT = RW_W * VH;  // doubles of one field's plane tile
-  static constexpr int DP = RW_W * DH;  // doubles of one dp plane
-  static constexpr int PT = RW_W * TY;  // doubles of one P plane tile (rows y0 .. y0+TY-1)
-  static constexpr size_t vel_bytes = (size_t)NS * 3 * VT * 8;
-  static constexpr size_t p_bytes = (size_t)NS * PT * 8;
-  static constexpr size_t dp_bytes = (size_t)NS * DP * 8;
+  // resident CTAs the register budget is sized for (FP32 state fits two
+  // CTAs of up to 11 warps without spilling; FP64 state only 8 warps)
+  static constexpr int MINB = (NT <= 256 || (sizeof(T) == 4 && NT <= 352)) ? 2 : 1;
+  static constexpr int VT = RW_W * VH;  // elements of one field's plane tile
+  static constexpr int DP = RW_W * DH;  // elements of one dp plane
+  static constexpr int PT = RW_W * TY;  // elements of one P plane tile (rows y0 .. y0+TY-1)
+  static constexpr size_t vel_bytes = (size_t)NS * 3 * VT * sizeof(T);
+  static constexpr size_t p_bytes = (size_t)NS * PT * sizeof(T);
+  static constexpr size_t dp_bytes = (size_t)NS * DP * sizeof(T);
   static constexpr size_t bar_bytes = 8 * NS;
   static constexpr size_t red_bytes = 8 * 32;
   static constexpr size_t total = vel_bytes + p_bytes + dp_bytes + bar_bytes + red_bytes + 16;
   static_assert(NS == 3, "the dp ring shares the slot index of the TMA ring (3 planes)");
-  static_assert((VT * 8) % 128 == 0 && (PT * 8) % 128 == 0, "TMA destinations must stay 128-byte aligned");
-  static_assert((DP * 8) % 16 == 0, "dp rows must stay 16-byte aligned");
+  static_assert((VT * sizeof(T)) % 128 == 0 && (PT * sizeof(T)) % 128 == 0, "TMA destinations must stay 128-byte aligned");
+  static_assert((DP * sizeof(T)) % 16 == 0, "dp rows must stay 16-byte aligned");
   static_assert(NW <= 32, "one reduction slot per warp");
 };
 
-__device__ __forceinline__ double2 lds2(const double* p) { return *reinterpret_cast<const double2*>(p); }
-__device__ __forceinline__ double shfl_up1(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
-__device__ __forceinline__ double shfl_down1(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+template <typename T> __device__ __forceinline__ pair_t<T> lds2(const T* p) {
+  return *reinterpret_cast<const pair_t<T>*>(p);
+}
+template <typename T> __device__ __forceinline__ void st2(T* p, T a, T b) {
+  *reinterpret_cast<pair_t<T>*>(p) = mk2<T>(a, b);
+}
+template <typename T> __device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <typename T> __device__ __forceinline__ T shfl_down1(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+// face_update of k_hsmac_tma for either field type: the contributions of the
+// two cells sharing a face in the order of the in-place sweep.
+template <typename T>
+__device__ __forceinline__ T face_update_t(T val, bool lower_first, bool ma, T da, bool mb, T db, T dci) {
+  const T ta = da * dci, tb = db * dci;
+  if (lower_first) {
+    val = ma ? val + ta : val;
+    val = mb ? val - tb : val;
+  } else {
+    val = mb ? val - tb : val;
+    val = ma ? val + ta : val;
+  }
+  return val;
+}
 
 // Per-lane (x) and per-warp (y) membership bits of one tile.
 struct RwBits {
@@ -87,21 +117,23 @@ struct RwBits {
 };
 
 
-// x0 (a tile's first output column) is odd: the pairs (x0-2+2l, x0-1+2l) and
-// the TMA box starting at x0-2 are then 16-byte aligned.  Work items are
+// x0 (a tile's first output column) puts x0-2 on a 16-byte boundary (x0 odd
+// in FP64, x0 = 3 mod 4 in FP32): the TMA boxes start there and every pair
+// (x0-2+2l, x0-1+2l) is aligned to its own size.  Work items are
 // (z chunk, tile column), chunk major, as in k_hsmac_tma.
-template <int TY, int NS>
-__global__ void __launch_bounds__(RwLayout<TY, NS>::NT, (RwLayout<TY, NS>::NT <= 256 ? 2 : 1))
+template <typename T, int TY, int NS>
+__global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::MINB)
     k_hsmac_rw(Ctx* __restrict__ ctx, Grid g, int set, const __grid_constant__ TensorMaps tm,
-               double* __restrict__ P, Box D, Box out, Box gb, int x_origin, int gx, int gy, int zc, int nitems,
+               T* __restrict__ P, Box D, Box out, Box gb, int x_origin, int gx, int gy, int zc, int nitems,
                HsmacCoef cf, double* __restrict__ partials, int finalize, int group_end) {
-  using L = RwLayout<TY, NS>;
+  using L = RwLayout<T, TY, NS>;
+  using T2 = pair_t<T>;
   constexpr int NT = L::NT, VT = L::VT, DP = L::DP, W = RW_W;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int PT = L::PT;
-  double* svel = (double*)smem_raw;                               // [NS][3][VH][W]
-  double* sP = (double*)(smem_raw + L::vel_bytes);                // [NS][TY][W]
-  double* sdp = (double*)(smem_raw + L::vel_bytes + L::p_bytes);  // [NS][DH][W]
+  T* svel = (T*)smem_raw;                               // [NS][3][VH][W]
+  T* sP = (T*)(smem_raw + L::vel_bytes);                // [NS][TY][W]
+  T* sdp = (T*)(smem_raw + L::vel_bytes + L::p_bytes);  // [NS][DH][W]
   uint64_t* bars = (uint64_t*)(smem_raw + L::vel_bytes + L::p_bytes + L::dp_bytes);
   double* red = (double*)(smem_raw + L::vel_bytes + L::p_bytes + L::dp_bytes + L::bar_bytes);
   int* last_flag = (int*)(red + 32);
@@ -113,13 +145,13 @@ __global__ void __launch_bounds__(RwLayout<TY, NS>::NT, (RwLayout<TY, NS>::NT <=
 
   if (!skip) {
     const int m0i = ctx->vphys[set][0], m1i = ctx->vphys[set][1], m2i = ctx->vphys[set][2];
-    double* Uo = (double*)ctx->vel[kSetSpare][0];
-    double* Vo = (double*)ctx->vel[kSetSpare][1];
-    double* Wo = (double*)ctx->vel[kSetSpare][2];
-    const double dxi = cf.dxi, dyi = cf.dyi, dzi = cf.dzi, dl = cf.dl, om = cf.omega;
-    const double dti = 1.0 / ctx->scal[0];
-    const int A = kAlignElems<double>;
-    const uint32_t plane_tx = (3u * VT + PT) * 8u;
+    T* Uo = (T*)ctx->vel[kSetSpare][0];
+    T* Vo = (T*)ctx->vel[kSetSpare][1];
+    T* Wo = (T*)ctx->vel[kSetSpare][2];
+    const T dxi = (T)cf.dxi, dyi = (T)cf.dyi, dzi = (T)cf.dzi, dl = (T)cf.dl, om = (T)cf.omega;
+    const T dti = (T)(1.0 / ctx->scal[0]);
+    const int A = kAlignElems<T>;
+    const uint32_t plane_tx = (3u * VT + PT) * (uint32_t)sizeof(T);
     if (tid == 0) {
       for (int q = 0; q < NS; q++) mbar_init(&bars[q], 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -140,7 +172,7 @@ __global__ void __launch_bounds__(RwLayout<TY, NS>::NT, (RwLayout<TY, NS>::NT <=
       auto issue = [&](int l) {  // plane s = kb-2+l into slot (load0+l) % NS
         const int li = load0 + l, slot = li % NS;
         mbar_arrive_expect_tx(&bars[slot], plane_tx);
-        double* base = svel + slot * 3 * VT;
+        T* base = svel + slot * 3 * VT;
         const int cz = kb - 2 + l + h - 1;
         tma_load_3d(base, &tm.vel[m0i], &bars[slot], cx, cy, cz);
         tma_load_3d(base + VT, &tm.vel[m1i], &bars[slot], cx, cy, cz);
@@ -195,11 +227,11 @@ __global__ void __launch_bounds__(RwLayout<TY, NS>::NT, (RwLayout<TY, NS>::NT <=
       // plane s): U, V (row j), V (row j-1), W and P of the plane; D0[q] = dp0 of
       // the colour-0 cell of the pair at that plane; DM[q] = the final dp pair
       // at s-1 computed at plane s; wb = W at s-2.
-      const double2 zero2 = make_double2(0.0, 0.0);
-      double2 Us2[2] = {zero2, zero2}, Vs2[2] = {zero2, zero2}, Vb2[2] = {zero2, zero2};
-      double2 Ws2[2] = {zero2, zero2}, Ps2[2] = {zero2, zero2}, DM[2] = {zero2, zero2};
-      double D0[2] = {0.0, 0.0};
-      double2 wb = zero2;
+      const T2 zero2 = mk2<T>(T(0), T(0));
+      T2 Us2[2] = {zero2, zero2}, Vs2[2] = {zero2, zero2}, Vb2[2] = {zero2, zero2};
+      T2 Ws2[2] = {zero2, zero2}, Ps2[2] = {zero2, zero2}, DM[2] = {zero2, zero2};
+      T D0[2] = {T(0), T(0)};
+      T2 wb = zero2;
       int sl = load0 % NS;  // ring slot of plane s (velocity, P and dp rings alike)
       uint32_t par = (uint32_t)((load0 / NS) & 1);
 
@@ -224,102 +256,102 @@ __global__ void __launch_bounds__(RwLayout<TY, NS>::NT, (RwLayout<TY, NS>::NT <=
         const bool y1 = bt.yrow && (ZF || (k1 >= kb && k1 <= ke));  // U, V, P of plane s-1
         const bool y2 = bt.yrow && (ZF || (k2 >= kb && k2 <= ke));  // W of plane s-2
         const int slm = sl == 0 ? NS - 1 : sl - 1;
-        const double* Vt = svel + sl * 3 * VT;
+        const T* Vt = svel + sl * 3 * VT;
         Us2[Q] = lds2(Vt + vofs);
         Vs2[Q] = lds2(Vt + VT + vofs);
         Vb2[Q] = lds2(Vt + VT + vofs - W);
         Ws2[Q] = lds2(Vt + 2 * VT + vofs);
         if (bt.yrow) Ps2[Q] = lds2(sP + sl * PT + pofs);
-        const double2 us = Us2[Q], vs = Vs2[Q], vbs = Vb2[Q], ws = Ws2[Q];
-        const double2 um = Us2[QM], vm = Vs2[QM], vbm = Vb2[QM], wm = Ws2[QM];
-        const double d0p = D0[QM];   // dp0 at s-1 of the pair's colour-0 cell there
-        const double2 dpb = DM[QM];  // final dp pair at s-2
-        double* dps = sdp + sl * DP + dofs;   // this row's pair, plane s
-        double* dpm = sdp + slm * DP + dofs;  // this row's pair, plane s-1
+        const T2 us = Us2[Q], vs = Vs2[Q], vbs = Vb2[Q], ws = Ws2[Q];
+        const T2 um = Us2[QM], vm = Vs2[QM], vbm = Vb2[QM], wm = Ws2[QM];
+        const T d0p = D0[QM];   // dp0 at s-1 of the pair's colour-0 cell there
+        const T2 dpb = DM[QM];  // final dp pair at s-2
+        T* dps = sdp + sl * DP + dofs;   // this row's pair, plane s
+        T* dpm = sdp + slm * DP + dofs;  // this row's pair, plane s-1
 
         // ---- phase X: dp0 at (A, s), dp1 at (A, s-1)
-        double d0 = 0.0, d1 = 0.0;
+        T d0 = T(0), d1 = T(0);
         {
-          double upA = 0.0, upM = 0.0;  // U[xL-1] at s and s-1, from the lane below
+          T upA = T(0), upM = T(0);  // U[xL-1] at s and s-1, from the lane below
           if constexpr (!R) {
             upA = shfl_up1(us.y);
             upM = shfl_up1(um.y);
           }
           // dp0 at s-1 of the x neighbour held by the adjacent lane (A+1 for R, A-1 for L)
-          const double d0x = R ? shfl_down1(d0p) : shfl_up1(d0p);
-          const double uA = R ? us.y : us.x, uAm = R ? us.x : upA;
-          const double vA = R ? vs.y : vs.x, vbA = R ? vbs.y : vbs.x;
-          const double wA = R ? ws.y : ws.x, wmA = R ? wm.y : wm.x;
+          const T d0x = R ? shfl_down1(d0p) : shfl_up1(d0p);
+          const T uA = R ? us.y : us.x, uAm = R ? us.x : upA;
+          const T vA = R ? vs.y : vs.x, vbA = R ? vbs.y : vbs.x;
+          const T wA = R ? ws.y : ws.x, wmA = R ? wm.y : wm.x;
           const bool inA = FULL || (bt.dy && (R ? bt.dR : bt.dL));
           const bool m0 = do0 && z_s && inA;
           const bool ownA = bt.owny && (FULL ? lane_out : (R ? bt.ownR : bt.ownL));
           if (m0) {
-            const double dudx = dxi * (-uAm + uA);
-            const double dvdy = dyi * (-vbA + vA);
-            const double dwdz = dzi * (-wmA + wA);
-            const double div = dudx + dvdy + dwdz;
+            const T dudx = dxi * (-uAm + uA);
+            const T dvdy = dyi * (-vbA + vA);
+            const T dwdz = dzi * (-wmA + wA);
+            const T div = dudx + dvdy + dwdz;
             d0 = -om * div * dl;
-            if (own_s && ownA) racc += div * div;
+            if (own_s && ownA) racc += (double)div * (double)div;
           }
           if (do0) dps[R ? 1 : 0] = d0;
           const bool m1 = do1 && z_m && bt.d1y && inA;
           if (m1) {
-            const double dyl = dpm[(R ? 1 : 0) - W], dyu = dpm[(R ? 1 : 0) + W];  // dp0 of rows j-1, j+1
-            double ul = R ? um.x : upM, ur = R ? um.y : um.x;
-            double vl = R ? vbm.y : vbm.x, vr = R ? vm.y : vm.x;
-            double wl = R ? wb.y : wb.x, wr = R ? wm.y : wm.x;
-            const double cl = (R ? d0p : d0x) * dxi, cr = (R ? d0x : d0p) * dxi;
-            const double cd = dyl * dyi, cu = dyu * dyi;
-            const double cb = (R ? dpb.y : dpb.x) * dzi, ct = d0 * dzi;
+            const T dyl = dpm[(R ? 1 : 0) - W], dyu = dpm[(R ? 1 : 0) + W];  // dp0 of rows j-1, j+1
+            T ul = R ? um.x : upM, ur = R ? um.y : um.x;
+            T vl = R ? vbm.y : vbm.x, vr = R ? vm.y : vm.x;
+            T wl = R ? wb.y : wb.x, wr = R ? wm.y : wm.x;
+            const T cl = (R ? d0p : d0x) * dxi, cr = (R ? d0x : d0p) * dxi;
+            const T cd = dyl * dyi, cu = dyu * dyi;
+            const T cb = (R ? dpb.y : dpb.x) * dzi, ct = d0 * dzi;
             ul = (FULL || (R ? bt.dL : bt.dLm)) ? ul + cl : ul;
             ur = (FULL || (R ? bt.dRp : bt.dR)) ? ur - cr : ur;
             vl = (FULL || bt.dym) ? vl + cd : vl;
             vr = (FULL || bt.dyp) ? vr - cu : vr;
             wl = z_b ? wl + cb : wl;
             wr = m0 ? wr - ct : wr;
-            const double dudx = dxi * (-ul + ur);
-            const double dvdy = dyi * (-vl + vr);
-            const double dwdz = dzi * (-wl + wr);
-            const double div = dudx + dvdy + dwdz;
+            const T dudx = dxi * (-ul + ur);
+            const T dvdy = dyi * (-vl + vr);
+            const T dwdz = dzi * (-wl + wr);
+            const T div = dudx + dvdy + dwdz;
             d1 = -om * div * dl;
-            if (own_m && ownA) racc += div * div;
+            if (own_m && ownA) racc += (double)div * (double)div;
           }
           if (do1 && bt.d1y && (FULL || (R ? bt.d1R : bt.d1L))) dpm[R ? 1 : 0] = d1;
         }
         D0[Q] = d0;
-        const double2 dm = R ? make_double2(d0p, d1) : make_double2(d1, d0p);  // final dp at s-1
+        const T2 dm = R ? mk2<T>(d0p, d1) : mk2<T>(d1, d0p);  // final dp at s-1
         DM[Q] = dm;
         if (__syncthreads_or(!ok)) return false;
         if (tid == 0 && l + NS < nplanes) issue(l + NS);  // every warp is past its reads of this slot
 
         // ---- phase Y: U, V, P at s-1 and W at s-2 of the pair
-        const double dN = shfl_down1(dm.x);  // dp(xR+1, s-1)
-        const double2 pv = Ps2[QM];          // P at s-1
+        const T dN = shfl_down1(dm.x);  // dp(xR+1, s-1)
+        const T2 pv = Ps2[QM];          // P at s-1
         const int64_t o1 = grow + (int64_t)k1 * g.pz;
         if (y1) {
-          const double2 dup = lds2(dpm + W);  // final dp of row j+1 at s-1
+          const T2 dup = lds2(dpm + W);  // final dp of row j+1 at s-1
           const bool mL = z_m && (FULL || (bt.dy && bt.dL)), mR = z_m && (FULL || (bt.dy && bt.dR));
           const bool mRp = z_m && (FULL || (bt.dy && bt.dRp));
           const bool upL = z_m && (FULL || (bt.dyp && bt.dL)), upR = z_m && (FULL || (bt.dyp && bt.dR));
           // the left cell is colour 0 at s-1 exactly when R
-          const double u0 = face_update(um.x, R, mL, dm.x, mR, dm.y, dxi);
-          const double u1 = face_update(um.y, !R, mR, dm.y, mRp, dN, dxi);
-          const double v0 = face_update(vm.x, R, mL, dm.x, upL, dup.x, dyi);
-          const double v1 = face_update(vm.y, !R, mR, dm.y, upR, dup.y, dyi);
-          const double p0 = mL ? pv.x + dm.x * dti : pv.x;
-          const double p1 = mR ? pv.y + dm.y * dti : pv.y;
+          const T u0 = face_update_t<T>(um.x, R, mL, dm.x, mR, dm.y, dxi);
+          const T u1 = face_update_t<T>(um.y, !R, mR, dm.y, mRp, dN, dxi);
+          const T v0 = face_update_t<T>(vm.x, R, mL, dm.x, upL, dup.x, dyi);
+          const T v1 = face_update_t<T>(vm.y, !R, mR, dm.y, upR, dup.y, dyi);
+          const T p0 = mL ? pv.x + dm.x * dti : pv.x;
+          const T p1 = mR ? pv.y + dm.y * dti : pv.y;
           if (FULL) {
             if (lane_out) {
-              *reinterpret_cast<double2*>(Uo + o1) = make_double2(u0, u1);
-              *reinterpret_cast<double2*>(Vo + o1) = make_double2(v0, v1);
-              *reinterpret_cast<double2*>(P + o1) = make_double2(p0, p1);  // interior: 1 <= k1 <= nz in ZF
+              st2<T>(Uo + o1, u0, u1);
+              st2<T>(Vo + o1, v0, v1);
+              st2<T>(P + o1, p0, p1);  // interior: 1 <= k1 <= nz in ZF
             }
           } else {
             const bool oy = bt.outy && k1 >= out.lo[2] && k1 <= out.hi[2];
             const bool oL = oy && bt.outL, oR = oy && bt.outR;
             if (oL && oR) {
-              *reinterpret_cast<double2*>(Uo + o1) = make_double2(u0, u1);
-              *reinterpret_cast<double2*>(Vo + o1) = make_double2(v0, v1);
+              st2<T>(Uo + o1, u0, u1);
+              st2<T>(Vo + o1, v0, v1);
             } else {
               if (oL) { Uo[o1] = u0; Vo[o1] = v0; }
               if (oR) { Uo[o1 + 1] = u1; Vo[o1 + 1] = v1; }
@@ -328,7 +360,7 @@ __global__ void __launch_bounds__(RwLayout<TY, NS>::NT, (RwLayout<TY, NS>::NT <=
             const bool pj = bt.inty && k1 >= 1 && k1 <= nz;
             const bool pL = pj && bt.intL, pR = pj && bt.intR;
             if (pL && pR) {
-              *reinterpret_cast<double2*>(P + o1) = make_double2(p0, p1);
+              st2<T>(P + o1, p0, p1);
             } else {
               if (pL) P[o1] = p0;
               if (pR) P[o1 + 1] = p1;
@@ -338,16 +370,16 @@ __global__ void __launch_bounds__(RwLayout<TY, NS>::NT, (RwLayout<TY, NS>::NT <=
         if (y2) {
           // W faces between planes s-2 and s-1; the left cell is colour 0 at s-2 exactly when !R
           const bool mxL = FULL || (bt.dy && bt.dL), mxR = FULL || (bt.dy && bt.dR);
-          const double w0 = face_update(wb.x, !R, z_b && mxL, dpb.x, z_m && mxL, dm.x, dzi);
-          const double w1 = face_update(wb.y, R, z_b && mxR, dpb.y, z_m && mxR, dm.y, dzi);
+          const T w0 = face_update_t<T>(wb.x, !R, z_b && mxL, dpb.x, z_m && mxL, dm.x, dzi);
+          const T w1 = face_update_t<T>(wb.y, R, z_b && mxR, dpb.y, z_m && mxR, dm.y, dzi);
           const int64_t o2 = o1 - g.pz;
           if (FULL) {
-            if (lane_out) *reinterpret_cast<double2*>(Wo + o2) = make_double2(w0, w1);
+            if (lane_out) st2<T>(Wo + o2, w0, w1);
           } else {
             const bool oy = bt.outy && k2 >= out.lo[2] && k2 <= out.hi[2];
             const bool oL = oy && bt.outL, oR = oy && bt.outR;
             if (oL && oR) {
-              *reinterpret_cast<double2*>(Wo + o2) = make_double2(w0, w1);
+              st2<T>(Wo + o2, w0, w1);
             } else {
               if (oL) Wo[o2] = w0;
               if (oR) Wo[o2 + 1] = w1;

@@ -83,38 +83,44 @@ struct FillArgs {
 };
 
 template <typename T>
-__global__ void k_fill_halo(const Ctx* __restrict__ ctx, Grid g, FillArgs fa, int r, int full, int64_t total) {
+__global__ void __launch_bounds__(256) k_fill_halo(const Ctx* __restrict__ ctx, Grid g, FillArgs fa, int r, int full,
+                                                   int64_t total) {
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
   const int wx = full ? nx + 2 * r : nx, wy = full ? ny + 2 * r : ny;
   const int bx = full ? 1 - r : 1, by = full ? 1 - r : 1;
-  const int64_t segA = (int64_t)2 * r * wx * wy;          // z slabs
-  const int64_t segB = (int64_t)2 * r * nz * wx;          // y slabs, k interior
+  const int segA = 2 * r * wx * wy;  // z slabs
+  const int segB = 2 * r * nz * wx;  // y slabs, k interior
+  const int r2 = 2 * r;
   T* f[4];
-  for (int q = 0; q < fa.nf; q++)
-    f[q] = (T*)(fa.set[q] >= 0 ? ctx->vel[fa.set[q]][fa.comp[q]] : fa.ptr[q]);
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    f[q] = q < fa.nf ? (T*)(fa.set[q] >= 0 ? ctx->vel[fa.set[q]][fa.comp[q]] : fa.ptr[q]) : nullptr;
+  // total < 2^31 (checked on the host): 32-bit index arithmetic
+  const int tot = (int)total;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
     int i, j, k;
     if (t < segA) {
-      int64_t u = t;
-      i = bx + (int)(u % wx); u /= wx;
-      j = by + (int)(u % wy); u /= wy;
-      int kk = (int)u;  // 0..2r-1
-      k = kk < r ? 1 - r + kk : nz + 1 + (kk - r);
+      int u = t;
+      i = bx + u % wx; u /= wx;
+      j = by + u % wy; u /= wy;
+      k = u < r ? 1 - r + u : nz + 1 + (u - r);
     } else if (t < segA + segB) {
-      int64_t u = t - segA;
-      i = bx + (int)(u % wx); u /= wx;
-      int jj = (int)(u % (2 * r)); u /= (2 * r);
-      k = 1 + (int)u;
+      int u = t - segA;
+      i = bx + u % wx; u /= wx;
+      const int jj = u % r2; u /= r2;
+      k = 1 + u;
       j = jj < r ? 1 - r + jj : ny + 1 + (jj - r);
     } else {
-      int64_t u = t - segA - segB;
-      int ii = (int)(u % (2 * r)); u /= (2 * r);
-      j = 1 + (int)(u % ny); u /= ny;
-      k = 1 + (int)u;
+      int u = t - segA - segB;
+      const int ii = u % r2; u /= r2;
+      j = 1 + u % ny; u /= ny;
+      k = 1 + u;
       i = ii < r ? 1 - r + ii : nx + 1 + (ii - r);
     }
     const int64_t dst = g.at(i, j, k), src = g.at(wrap1(i, nx), wrap1(j, ny), wrap1(k, nz));
-    for (int q = 0; q < fa.nf; q++) f[q][dst] = f[q][src];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (q < fa.nf) f[q][dst] = f[q][src];
   }
 }
 
@@ -379,7 +385,8 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-constexpr int kGridBarrierSpins = 1 << 22;  // x >= 32 ns sleeps: > 0.1 s
+constexpr long long kGridBarrierCycles = 200000000;  // ~0.1 s at 2 GHz
+constexpr int kGridBarrierPolls = 1 << 24;
 
 __device__ __forceinline__ bool grid_barrier(Ctx* ctx, unsigned int nblocks, int* flag_sh) {
   __syncthreads();
@@ -392,13 +399,12 @@ __device__ __forceinline__ bool grid_barrier(Ctx* ctx, unsigned int nblocks, int
       __threadfence();
       atomicAdd(&ctx->gbar_gen, 1u);
     } else {
-      int it = 0;
-      while (ld_acquire_gpu(&ctx->gbar_gen) == gen) {
-        if (++it > kGridBarrierSpins) {
+      const long long t0 = clock64();
+      for (int it = 0; ld_acquire_gpu(&ctx->gbar_gen) == gen; it++) {
+        if (it > kGridBarrierPolls || clock64() - t0 > kGridBarrierCycles) {
           ok = 0;
           break;
         }
-        __nanosleep(32);
       }
     }
     __threadfence();
@@ -414,41 +420,21 @@ struct FaceSet {
   Box f[6];
 };
 
-// In-place colour phase of one face slab for the cell with flat index t among
-// the colour's cells (the k_hsmac_phase mapping); returns whether a cell was
-// updated and its div in *div.  Loads bypass L1 (__ldcg): after a grid
-// barrier a block reads cells that other blocks have just written.
-template <typename T>
-__device__ __forceinline__ bool face_cell(const Grid& g, const Box& b, int64_t t, int color, int coloring, T* U, T* V,
-                                          T* W, T* P, T dxi, T dyi, T dzi, T dl, T om, T dti, T* div_out, bool* in_r) {
+// Cell with flat index t among the cells of colour `color` of a face slab (the
+// k_hsmac_phase mapping): false when the index maps to no such cell.
+__device__ __forceinline__ bool face_locate(const Grid& g, const Box& b, int t, int color, int coloring, int64_t* c,
+                                            bool* in_r) {
   const int lx = b.len(0), ly = b.len(1);
   const int hx = (lx + 1) / 2;
-  int64_t u = t;
-  const int m = (int)(u % hx); u /= hx;
-  const int j = b.lo[1] + (int)(u % ly); u /= ly;
-  const int k = b.lo[2] + (int)u;
+  int u = t;
+  const int m = u % hx; u /= hx;
+  const int j = b.lo[1] + u % ly; u /= ly;
+  const int k = b.lo[2] + u;
   const int a = b.lo[0];
   const int i = a + 2 * m + ((j + k - a + color) & 1);
   if (i > b.hi[0]) return false;
   if (cell_color(coloring, i, j, k) != color) return false;
-  const int64_t c = g.at(i, j, k), sy = g.px, sz = g.pz;
-  const T u0 = __ldcg(U + c - 1), u1 = __ldcg(U + c);
-  const T v0 = __ldcg(V + c - sy), v1 = __ldcg(V + c);
-  const T w0 = __ldcg(W + c - sz), w1 = __ldcg(W + c);
-  const T p0 = __ldcg(P + c);
-  const T dudx = dxi * diff1_o2_at_half<T>(u0, u1);
-  const T dvdy = dyi * diff1_o2_at_half<T>(v0, v1);
-  const T dwdz = dzi * diff1_o2_at_half<T>(w0, w1);
-  const T div = dudx + dvdy + dwdz;
-  const T dp = -om * div * dl;
-  P[c] = p0 + dp * dti;
-  U[c - 1] = u0 - dp * dxi;
-  U[c] = u1 + dp * dxi;
-  V[c - sy] = v0 - dp * dyi;
-  V[c] = v1 + dp * dyi;
-  W[c - sz] = w0 - dp * dzi;
-  W[c] = w1 + dp * dzi;
-  *div_out = div;
+  *c = g.at(i, j, k);
   *in_r = i >= 1 && i <= g.n[0] + 1 && j >= 1 && j <= g.n[1] + 1 && k >= 1 && k <= g.n[2] + 1;
   return true;
 }
@@ -473,26 +459,61 @@ __global__ void __launch_bounds__(256) k_hsmac_faces(Ctx* __restrict__ ctx, Grid
   T* W = (T*)ctx->vel[set][2];
   const T dxi = (T)cf.dxi, dyi = (T)cf.dyi, dzi = (T)cf.dzi, dl = (T)cf.dl, om = (T)cf.omega;
   const T dti = (T)(1.0 / ctx->scal[0]);
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int stride = gridDim.x * blockDim.x;
   double acc = 0.0;
   bool ok = true;
   for (int p = 0; p < 6; p++) {
     const int color = p & 1;
     const Box& ba = fs.f[p & ~1];
     const Box& bb = fs.f[(p & ~1) + 1];
-    auto ncell = [](const Box& b) -> int64_t {
+    auto ncell = [](const Box& b) -> int {  // a face slab holds < 2^31 cells (checked on the host)
       if (b.lo[0] > b.hi[0] || b.lo[1] > b.hi[1] || b.lo[2] > b.hi[2]) return 0;
-      return (int64_t)((b.len(0) + 1) / 2) * b.len(1) * b.len(2);
+      return ((b.len(0) + 1) / 2) * b.len(1) * b.len(2);
     };
-    const int64_t na = ncell(ba), nt = na + ncell(bb);
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += stride) {
-      T div;
-      bool in_r;
-      const bool upd = t < na ? face_cell<T>(g, ba, t, color, cf.coloring, U, V, W, P, dxi, dyi, dzi, dl, om, dti,
-                                             &div, &in_r)
-                              : face_cell<T>(g, bb, t - na, color, cf.coloring, U, V, W, P, dxi, dyi, dzi, dl, om,
-                                             dti, &div, &in_r);
-      if (upd && in_r) acc += (double)div * (double)div;
+    const int na = ncell(ba), nt = na + ncell(bb);
+    // Cells of one colour share no face, so the KB cells a thread takes per
+    // round are independent: all their loads are issued before any store.
+    // Loads bypass L1 (__ldcg): after a grid barrier a block reads cells that
+    // other blocks have just written.
+    constexpr int KB = 4;
+    for (int t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < nt; t0 += KB * stride) {
+      int64_t c[KB];
+      bool v[KB], inr[KB];
+      T u0[KB], u1[KB], v0[KB], v1[KB], w0[KB], w1[KB], p0[KB];
+#pragma unroll
+      for (int q = 0; q < KB; q++) {
+        const int t = t0 + q * stride;
+        c[q] = 0;
+        inr[q] = false;
+        v[q] = t < nt && (t < na ? face_locate(g, ba, t, color, cf.coloring, &c[q], &inr[q])
+                                 : face_locate(g, bb, t - na, color, cf.coloring, &c[q], &inr[q]));
+        if (v[q]) {
+          const int64_t cc = c[q], sy = g.px, sz = g.pz;
+          u0[q] = __ldcg(U + cc - 1); u1[q] = __ldcg(U + cc);
+          v0[q] = __ldcg(V + cc - sy); v1[q] = __ldcg(V + cc);
+          w0[q] = __ldcg(W + cc - sz); w1[q] = __ldcg(W + cc);
+          p0[q] = __ldcg(P + cc);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < KB; q++) {
+        if (!v[q]) continue;
+        const int64_t cc = c[q], sy = g.px, sz = g.pz;
+        // hsmac.jl:1-35, the reference's operation order
+        const T dudx = dxi * diff1_o2_at_half<T>(u0[q], u1[q]);
+        const T dvdy = dyi * diff1_o2_at_half<T>(v0[q], v1[q]);
+        const T dwdz = dzi * diff1_o2_at_half<T>(w0[q], w1[q]);
+        const T div = dudx + dvdy + dwdz;
+        const T dp = -om * div * dl;
+        P[cc] = p0[q] + dp * dti;
+        U[cc - 1] = u0[q] - dp * dxi;
+        U[cc] = u1[q] + dp * dxi;
+        V[cc - sy] = v0[q] - dp * dyi;
+        V[cc] = v1[q] + dp * dyi;
+        W[cc - sz] = w0[q] - dp * dzi;
+        W[cc] = w1[q] + dp * dzi;
+        if (inr[q]) acc += (double)div * (double)div;
+      }
     }
     if (p < 5 && !grid_barrier(ctx, gridDim.x, &flag)) {
       if (threadIdx.x == 0) ctx->wait_error = 1;

@@ -10,7 +10,7 @@ from lcs_b200 import _abi
 def make_config(n=16, *, mode=_abi.MODE_FLOW_PARTICLE, h=3, time_blocking=True, overlap=True,
                 coloring=_abi.COLORING_RED_BLACK_FAST, block=0, omega=1.7, epsp=1e-3, itrmin=6, itrmax=6,
                 forcing=_abi.FORCING_NO, power=1.0, energy=1.0, kmin=1, kmax=2, coarse=4, Re=1.0,
-                species=(), cfl=0.3, dtmax=0.01, graphs=0, dims=None):
+                species=(), cfl=0.3, dtmax=0.01, graphs=0, dims=None, precision=_abi.PRECISION_FP64):
     """An lcs_config; defaults follow the reference's unit tests (test/test_flows.jl:11-21,
     FlowParams(1,1,1), HSMAC(.., RedBlackFast, 1.7, 1e-3, 6, 6))."""
     c = _abi.Config()
@@ -32,7 +32,7 @@ def make_config(n=16, *, mode=_abi.MODE_FLOW_PARTICLE, h=3, time_blocking=True, 
         c.species[s].gravity = sp.get("gravity", 0.0)
         c.species[s].density_ratio = sp.get("density_ratio", 1.0)
         c.species[s].drag = sp.get("drag", _abi.DRAG_LINEAR)
-    c.precision = _abi.PRECISION_FP64
+    c.precision = precision
     c.device = 0
     c.use_graphs = graphs
     return c

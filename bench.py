@@ -76,10 +76,29 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def make_run_config(name, seed=0):
+def make_run_config(name, seed=0, precision=None):
     w = WORKLOADS[name]
-    d = lcfg.workload(w["n"], w["nu"], w["forcing"], w["taups"], w["counts"], seed=seed, precision=w["precision"])
+    d = lcfg.workload(w["n"], w["nu"], w["forcing"], w["taups"], w["counts"], seed=seed,
+                      precision=precision or w["precision"])
     return lcfg.from_dict(d), w
+
+
+def time_form(workload, precision, steps, seed, device):
+    """Device time of `steps` graph-replayed steps of another precision form on
+    the same workload and inputs (after one warm-up step)."""
+    from lcs_b200 import Engine
+
+    rc, w = make_run_config(workload, seed=seed, precision=precision)
+    rc.abi.device = device
+    rc.abi.use_graphs = 1
+    flow, parts = host_inputs(rc, pinned=False)
+    eng = Engine(rc.abi)
+    load_engine(eng, rc, flow, parts)
+    eng.step(1)
+    eng.synchronize()
+    _, ms = eng.step_timed(steps)
+    eng.close()
+    return ms
 
 
 def host_inputs(rc, pinned=False):
@@ -249,7 +268,7 @@ def run_b200(args):
     world, rank, local = dist_setup()
     from lcs_b200 import Engine
 
-    rc, w = make_run_config(args.workload, seed=rank)
+    rc, w = make_run_config(args.workload, seed=rank, precision=args.precision)
     rc.abi.device = local if world > 1 else int(os.environ.get("LCS_DEVICE", "0"))
     rc.abi.use_graphs = 1
     n3 = float(np.prod(rc.dims))
@@ -311,6 +330,18 @@ def run_b200(args):
     e2e_s = reduce_max(time.perf_counter() - t0, world)
     h2d1, d2h1 = eng.transfer_stats()
     e2e_value = world * n3 * e2e_steps / e2e_s / 1e6
+    eng.close()
+
+    # the other precision form on the same workload and seed (FP32-mixed beside FP64)
+    forms = None
+    if not args.no_forms:
+        other = "fp32-mixed" if args.precision == "fp64" else "fp64"
+        k = max(1, min(args.steps, 5))
+        ms_o = reduce_max(time_form(args.workload, other, k, rank, rc.abi.device), world)
+        v_o = world * n3 * k / (ms_o / 1e3) / 1e6
+        forms = {args.precision: {"value": value, "ms_per_step": ms_max / args.steps},
+                 other: {"value": v_o, "ms_per_step": ms_o / k, "steps": k}}
+        forms["fp32_mixed_vs_fp64"] = forms["fp32-mixed"]["value"] / forms["fp64"]["value"]
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -327,12 +358,13 @@ def run_b200(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64",
+            "dtype": "f64" if args.precision == "fp64" else "f32 (FP64 residuals, reductions, positions)",
             "data": "synthetic (seeded spectral field, uniform random particles)",
             "config": {"workload": args.workload, "n": rc.dims[0], "particles": int(np_tot),
                        "species": len(w["counts"]), "forcing": w["forcing"]["kind"], "hsmac_itrmax": 300,
                        "hsmac_rms_div_tol": 1e-8, "l2": "inputs larger than L2 (144 MB per field)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "precision": args.precision},
             "particle_steps_per_s": pvalue,
             "hsmac_sweeps_per_step": statistics.mean(sweeps) if sweeps else None,
             "gpu_launches": int(launches),
@@ -346,9 +378,9 @@ def run_b200(args):
                     "h2d_bytes_per_step": (h2d1 - h2d0) / e2e_steps, "d2h_bytes_per_step": (d2h1 - d2h0) / e2e_steps,
                     "steps": e2e_steps, "path": "upload + per-step lcs_timestep/lcs_evolve + download"},
             "cpu_baseline": ({k: base[k] for k in ("value", "unit", "cores", "kind", "sample")} if base else None),
+            "precision_forms": forms,
         }
         print(json.dumps(line), flush=True)
-    eng.close()
     barrier(world)
     return 0
 
@@ -361,6 +393,8 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rc256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["fp64", "fp32-mixed"], default="fp64")
+    ap.add_argument("--no-forms", action="store_true", help="skip timing the other precision form")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

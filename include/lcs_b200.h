@@ -222,6 +222,95 @@ LCS_API int lcs_launch_count(lcs_handle* h, int64_t* launches);
 LCS_API int lcs_transfer_stats(lcs_handle* h, int64_t* h2d_bytes, int64_t* d2h_bytes);
 LCS_API int lcs_synchronize(lcs_handle* h);
 
+/* ---- asynchronous steps (no reference counterpart) ----------------------
+ * For hosts that drive many handles at once (the batching and serving forms
+ * below, or a Julia task per handle).  lcs_step_begin enqueues nsteps
+ * (1..LCS_MAX_ASYNC_STEPS) device-resident steps, as lcs_step runs them, on
+ * the handle's stream and returns at once; lcs_step_poll reports whether they
+ * have finished without blocking; lcs_step_finish waits for them and fills
+ * logs[nsteps] (may be NULL).  Between begin and finish the handle accepts no
+ * other call but poll (ESTATE). */
+#define LCS_MAX_ASYNC_STEPS 4096
+LCS_API int lcs_step_begin(lcs_handle* h, int32_t nsteps);
+LCS_API int lcs_step_poll(lcs_handle* h, int32_t* done);
+LCS_API int lcs_step_finish(lcs_handle* h, lcs_log* logs);
+/* Device bytes the handle holds (its pool), as lcs_footprint predicts. */
+LCS_API int lcs_device_bytes(lcs_handle* h, int64_t* bytes);
+
+/* ---- batching form (no reference counterpart) ---------------------------
+ * An ensemble of independent runs with uneven grid sizes, particle counts and
+ * parameters, advanced together: lcs_batch_step enqueues every member's steps
+ * (each a CUDA-graph replay on the member's own stream) before waiting for any,
+ * so the members' kernels overlap on the GPU.  Each member computes exactly
+ * what it computes alone.  Members are ordinary handles (lcs_batch_member) for
+ * uploads, downloads and single-member calls between batch steps; the batch
+ * owns and destroys them.  logs is member-major: logs[i * nsteps + q]. */
+typedef struct lcs_batch lcs_batch;
+LCS_API int lcs_batch_create(const lcs_config* members, int32_t m, lcs_batch** out);
+LCS_API int lcs_batch_size(const lcs_batch* b, int32_t* m);
+LCS_API int lcs_batch_member(lcs_batch* b, int32_t i, lcs_handle** h);
+LCS_API int lcs_batch_step(lcs_batch* b, int32_t nsteps, lcs_log* logs);
+LCS_API void lcs_batch_destroy(lcs_batch* b);
+
+/* ---- serving form (no reference counterpart) ----------------------------
+ * A request loop with continuous batching.  Requests (a config, its initial
+ * state and a step count) are queued by lcs_server_submit.  The server's
+ * scheduler thread admits queued requests, oldest first, whenever a slot is
+ * free and the predicted device bytes of the admitted runs (lcs_footprint)
+ * stay within hbm_budget_bytes; it keeps each admitted run's state on the
+ * device, advances every admitted run by up to steps_per_slice steps at a
+ * time with the asynchronous steps above (their work overlaps on the GPU),
+ * and retires finished runs, whose final state it downloads, freeing their
+ * memory for the next admissions.  A run gives the same result alone and in
+ * the mix.  The submit copies the inputs: the caller's arrays may be freed on
+ * return. */
+typedef struct lcs_server lcs_server;
+typedef struct lcs_server_config {
+  int32_t device;
+  int32_t max_active;        /* admitted runs at most (slots) */
+  int32_t steps_per_slice;   /* steps enqueued per run per scheduling round (1..LCS_MAX_ASYNC_STEPS) */
+  int32_t _pad;
+  int64_t hbm_budget_bytes;  /* admitted runs' lcs_footprint sum at most */
+} lcs_server_config;
+typedef struct lcs_species_state {  /* one species' particles, n = config.species[s].nvalid */
+  const int64_t* ids;              /* may be NULL: ids 1..n */
+  const double *diam, *x, *y, *z, *u, *v, *w;
+} lcs_species_state;
+typedef struct lcs_request {
+  lcs_config config;               /* use_graphs is forced on; device is the server's */
+  const double *U, *V, *W, *P;     /* interior n^3 each, x fastest */
+  lcs_species_state species[LCS_MAX_SPECIES];
+  int32_t interp_velocity;         /* 1: particle velocity := fluid velocity at the particle */
+  int32_t _pad;
+  int64_t nsteps;                  /* timestep! + evolve! repetitions */
+} lcs_request;
+typedef struct lcs_species_out { double *x, *y, *z, *u, *v, *w; } lcs_species_out;  /* NULL: skipped */
+enum lcs_request_state { LCS_REQ_QUEUED = 0, LCS_REQ_RUNNING = 1, LCS_REQ_DONE = 2, LCS_REQ_FAILED = 3 };
+typedef struct lcs_server_stats {
+  int64_t submitted, completed, failed, queued, active;
+  int64_t bytes_in_use, peak_bytes_in_use;
+  double p50_latency_s, p99_latency_s;   /* submit -> result ready, over completed requests */
+  double mean_latency_s, busy_s;         /* busy_s: seconds with at least one admitted run */
+} lcs_server_stats;
+LCS_API int lcs_server_create(const lcs_server_config* c, lcs_server** out);
+LCS_API int lcs_server_submit(lcs_server* s, const lcs_request* r, int64_t* ticket);
+/* state: enum lcs_request_state; steps_done may be NULL. */
+LCS_API int lcs_server_poll(lcs_server* s, int64_t ticket, int32_t* state, int64_t* steps_done);
+/* Copies a finished request's final state (any pointer may be NULL; species
+ * out[config.n_species]), its last step log and its latency (seconds from
+ * submit to completion).  FAILED requests return their error code. */
+LCS_API int lcs_server_result(lcs_server* s, int64_t ticket, double* U, double* V, double* W, double* P,
+                              lcs_species_out* species, lcs_log* last_log, double* latency_s);
+/* Forgets a finished request (its stored result). */
+LCS_API int lcs_server_release(lcs_server* s, int64_t ticket);
+LCS_API int lcs_server_stats_get(lcs_server* s, lcs_server_stats* out);
+/* Blocks until every submitted request is DONE or FAILED, or timeout_s passes (ETIMEDOUT). */
+LCS_API int lcs_server_drain(lcs_server* s, double timeout_s);
+/* Stops the scheduler, finishing nothing further, and frees everything. */
+LCS_API void lcs_server_destroy(lcs_server* s);
+/* Message of the last failing server or batch call (thread-local). */
+LCS_API const char* lcs_serve_last_error(void);
+
 /* ---- allocation-free variant --------------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library
  * call cudaMalloc: code recording a CUDA stream capture, or a process whose

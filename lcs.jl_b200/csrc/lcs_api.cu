@@ -150,6 +150,21 @@ int lcs_timestep(lcs_handle* h, double* dt) { H(h); if (!dt) return LCS_EINVAL; 
 int lcs_evolve(lcs_handle* h, double dt, lcs_log* log) { H(h); return h->e->evolve(dt, log); }
 int lcs_step(lcs_handle* h, int32_t n, lcs_log* logs) { H(h); return h->e->step(n, logs); }
 int lcs_step_timed(lcs_handle* h, int32_t n, lcs_log* logs, double* ms) { H(h); return h->e->step_timed(n, logs, ms); }
+int lcs_step_begin(lcs_handle* h, int32_t n) { H(h); return h->e->step_begin(n); }
+int lcs_step_poll(lcs_handle* h, int32_t* done) {
+  H(h);
+  int d = 0;
+  const int rc = h->e->step_poll(&d);
+  if (done) *done = d;
+  return rc;
+}
+int lcs_step_finish(lcs_handle* h, lcs_log* logs) { H(h); return h->e->step_finish(logs); }
+int lcs_device_bytes(lcs_handle* h, int64_t* bytes) {
+  H(h);
+  if (!bytes) return LCS_EINVAL;
+  *bytes = h->e->device_bytes();
+  return LCS_OK;
+}
 int lcs_transfer_stats(lcs_handle* h, int64_t* a, int64_t* b) { H(h); return h->e->transfer_stats(a, b); }
 int lcs_synchalo(lcs_handle* h, int32_t mask, int32_t r, int32_t full) { H(h); return h->e->synchalo(mask, r, full); }
 int lcs_flow_rhs(lcs_handle* h, int32_t stage) { H(h); return h->e->rhs(stage); }

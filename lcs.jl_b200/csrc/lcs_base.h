@@ -30,6 +30,11 @@ struct EngineBase {
   virtual int evolve(double dt, lcs_log* log) = 0;
   virtual int step(int nsteps, lcs_log* logs) = 0;
   virtual int step_timed(int nsteps, lcs_log* logs, double* ms) = 0;
+  // asynchronous steps: enqueue, query without blocking, collect
+  virtual int step_begin(int nsteps) = 0;
+  virtual int step_poll(int* done) = 0;
+  virtual int step_finish(lcs_log* logs) = 0;
+  virtual int64_t device_bytes() const = 0;
   virtual int transfer_stats(int64_t* h2d, int64_t* d2h) = 0;
   virtual int synchalo(int mask, int r, int full) = 0;
   virtual int rhs(int stage) = 0;

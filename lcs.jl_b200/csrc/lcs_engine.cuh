@@ -163,6 +163,11 @@ class Engine : public EngineBase {
   std::vector<Tot> totals;
   // host-pinned mirrors
   Ctx* hctx = nullptr;
+  StepLog* hlogs = nullptr;  // staging of the step-log ring for asynchronous steps
+  cudaEvent_t async_ev = nullptr;
+  int async_pending = 0;      // steps enqueued by step_begin and not yet collected
+  long long host_step = 0;    // the device's step counter as last read (valid when host_step_known)
+  bool host_step_known = false;
   // graphs
   cudaGraphExec_t step_exec = nullptr, evolve_exec = nullptr;
   cudaGraph_t step_graph = nullptr, evolve_graph = nullptr;
@@ -181,6 +186,8 @@ class Engine : public EngineBase {
     for (auto& r : recs) { event_pool.push_back(r.a); event_pool.push_back(r.b); }
     for (auto e : event_pool) cudaEventDestroy(e);
     if (hctx) cudaFreeHost(hctx);
+    if (hlogs) cudaFreeHost(hlogs);
+    if (async_ev) cudaEventDestroy(async_ev);
     if (pool) cudaFree(pool);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -198,6 +205,8 @@ class Engine : public EngineBase {
       return fail(LCS_ENOMEM, "cudaMalloc of %zu bytes failed: %s", plan.bytes, cudaGetErrorString(e));
     }
     LCS_CUDA(cudaMallocHost(&hctx, sizeof(Ctx)));
+    LCS_CUDA(cudaMallocHost(&hlogs, (size_t)plan.logs_cap * sizeof(StepLog)));
+    LCS_CUDA(cudaEventCreateWithFlags(&async_ev, cudaEventDisableTiming));
     for (int s = 0; s < 3; s++)
       for (int q = 0; q < 3; q++) vel0[s][q] = pool + plan.off_vel[s][q];
     P = (T*)(pool + plan.off_P);
@@ -733,6 +742,8 @@ class Engine : public EngineBase {
   int read_ctx() {
     LCS_TRY(copy(hctx, dctx, sizeof(Ctx), cudaMemcpyDeviceToHost));
     LCS_CUDA(cudaStreamSynchronize(stream));
+    host_step = hctx->step;
+    host_step_known = true;
     return LCS_OK;
   }
 
@@ -1037,9 +1048,12 @@ class Engine : public EngineBase {
     return LCS_OK;
   }
   int set_state(int64_t step, double t) override {
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
     LCS_TRY(set_scalar(&dctx->t, t));
     LCS_TRY(copy(&dctx->step, &step, sizeof(long long), cudaMemcpyHostToDevice));
     LCS_CUDA(cudaStreamSynchronize(stream));
+    host_step = step;
+    host_step_known = true;
     return LCS_OK;
   }
   int get_state(int64_t* step, double* t) override {
@@ -1065,6 +1079,8 @@ class Engine : public EngineBase {
   }
   int evolve(double dt, lcs_log* log) override {
     LCS_TRY(check_flow());
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    host_step_known = false;  // the step counter advances on the device
     if (!(dt > 0) || !std::isfinite(dt)) return fail(LCS_EINVAL, "dt must be finite and positive");
     LCS_TRY(set_scalar(&dctx->dt, dt));
     if (cfg.use_graphs && !prof) {
@@ -1089,8 +1105,62 @@ class Engine : public EngineBase {
     if (d2h) *d2h = d2h_bytes;
     return LCS_OK;
   }
+  int64_t device_bytes() const override { return (int64_t)plan.bytes; }
+
+  // Asynchronous steps (the batch and the server drive many handles at once):
+  // step_begin enqueues nsteps graph replays of the step, then copies of the
+  // context and of those steps' log entries into pinned memory, and an event;
+  // step_poll tests the event; step_finish waits for it and returns the logs.
+  int step_begin(int nsteps) override {
+    LCS_TRY(check_flow());
+    if (async_pending) return fail(LCS_ESTATE, "steps are already in flight on this handle");
+    if (nsteps < 1 || nsteps > plan.logs_cap) return fail(LCS_EINVAL, "nsteps must be in 1..%lld", (long long)plan.logs_cap);
+    if (prof) return fail(LCS_ESTATE, "asynchronous steps do not run with profiling on");
+    if (!host_step_known) LCS_TRY(read_ctx());
+    LCS_TRY(build_step_graph());
+    for (int q = 0; q < nsteps; q++) {
+      LCS_CUDA(cudaGraphLaunch(step_exec, stream));
+      launches += graph_launches_per_step;
+    }
+    LCS_TRY(copy(hctx, dctx, sizeof(Ctx), cudaMemcpyDeviceToHost));
+    const int64_t cap = plan.logs_cap, i0 = host_step % cap;  // ring index of step host_step + 1
+    const int64_t n1 = std::min<int64_t>(nsteps, cap - i0);
+    LCS_TRY(copy(hlogs + i0, dlogs + i0, (size_t)n1 * sizeof(StepLog), cudaMemcpyDeviceToHost));
+    if (n1 < nsteps) LCS_TRY(copy(hlogs, dlogs, (size_t)(nsteps - n1) * sizeof(StepLog), cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaEventRecord(async_ev, stream));
+    async_pending = nsteps;
+    return LCS_OK;
+  }
+  int step_poll(int* done) override {
+    if (!done) return fail(LCS_EINVAL, "null output");
+    if (!async_pending) return fail(LCS_ESTATE, "no steps in flight on this handle");
+    const cudaError_t q = cudaEventQuery(async_ev);
+    if (q == cudaErrorNotReady) {
+      *done = 0;
+      return LCS_OK;
+    }
+    LCS_CUDA(q);
+    *done = 1;
+    return LCS_OK;
+  }
+  int step_finish(lcs_log* logs) override {
+    if (!async_pending) return fail(LCS_ESTATE, "no steps in flight on this handle");
+    const int n = async_pending;
+    async_pending = 0;
+    LCS_CUDA(cudaEventSynchronize(async_ev));
+    if (hctx->wait_error) return fail(LCS_ETIMEDOUT, "a bounded device wait (TMA tile load or grid barrier) ran out");
+    if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt near step %lld", (long long)hctx->step);
+    if (hctx->step != host_step + n) return fail(LCS_ECUDA, "step counter %lld, expected %lld", (long long)hctx->step,
+                                                 (long long)(host_step + n));
+    if (logs)
+      for (int q = 0; q < n; q++) fill_log(hlogs[(host_step + q) % plan.logs_cap], &logs[q]);
+    host_step += n;
+    return LCS_OK;
+  }
+
   int step_impl(int nsteps, lcs_log* logs, double* ms) {
     LCS_TRY(check_flow());
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
     if (nsteps < 0) return fail(LCS_EINVAL, "nsteps < 0");
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (ms) {

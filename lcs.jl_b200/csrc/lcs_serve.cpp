@@ -1,0 +1,530 @@
+// lcs_serve.cpp -- the batching and serving forms (no reference counterpart),
+// written against the public C ABI of include/lcs_b200.h only: a batch or a
+// server drives ordinary handles the way any host program could.
+//
+// Batch: every member's steps are enqueued (graph replays on the member's own
+// stream, lcs_step_begin) before any is waited for, so the members' kernels
+// run concurrently on the GPU; a member's arithmetic is exactly its solo run.
+//
+// Server: a scheduler thread owns every device call.  It admits queued
+// requests oldest first while a slot is free and the admitted runs' predicted
+// device bytes (lcs_footprint, the pool each handle allocates) fit the budget,
+// then keeps a slice of steps in flight for every admitted run and retires
+// finished runs (final state downloaded, handle destroyed, bytes returned).
+// User threads only touch host-side queues and results, under a mutex.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/lcs_b200.h"
+
+namespace {
+
+thread_local std::string t_err;
+
+int serve_fail(int rc, const std::string& msg) {
+  t_err = msg;
+  return rc;
+}
+
+std::string handle_error(const lcs_handle* h) {
+  const char* m = lcs_last_error(h);
+  return m ? std::string(m) : std::string();
+}
+
+using Clock = std::chrono::steady_clock;
+
+}  // namespace
+
+// ------------------------------------------------------------------ batch
+struct lcs_batch {
+  std::vector<lcs_handle*> members;
+};
+
+extern "C" {
+
+const char* lcs_serve_last_error(void) { return t_err.c_str(); }
+
+int lcs_batch_create(const lcs_config* members, int32_t m, lcs_batch** out) {
+  if (!out) return serve_fail(LCS_EINVAL, "null output");
+  *out = nullptr;
+  if (!members || m < 1) return serve_fail(LCS_EINVAL, "a batch needs at least one member config");
+  std::unique_ptr<lcs_batch> b(new lcs_batch);
+  for (int32_t i = 0; i < m; i++) {
+    lcs_config c = members[i];
+    c.use_graphs = 1;  // members run their steps as graph replays
+    lcs_handle* h = nullptr;
+    const int rc = lcs_create(&c, &h);
+    if (rc != LCS_OK) {
+      const std::string why = handle_error(nullptr);
+      for (lcs_handle* q : b->members) lcs_destroy(q);
+      return serve_fail(rc, "batch member " + std::to_string(i) + ": " + why);
+    }
+    b->members.push_back(h);
+  }
+  *out = b.release();
+  return LCS_OK;
+}
+
+int lcs_batch_size(const lcs_batch* b, int32_t* m) {
+  if (!b || !m) return serve_fail(LCS_EINVAL, "null argument");
+  *m = (int32_t)b->members.size();
+  return LCS_OK;
+}
+
+int lcs_batch_member(lcs_batch* b, int32_t i, lcs_handle** h) {
+  if (!b || !h) return serve_fail(LCS_EINVAL, "null argument");
+  if (i < 0 || i >= (int32_t)b->members.size()) return serve_fail(LCS_EINVAL, "member index out of range");
+  *h = b->members[i];
+  return LCS_OK;
+}
+
+int lcs_batch_step(lcs_batch* b, int32_t nsteps, lcs_log* logs) {
+  if (!b) return serve_fail(LCS_EINVAL, "null batch");
+  if (nsteps < 0) return serve_fail(LCS_EINVAL, "nsteps < 0");
+  const int32_t m = (int32_t)b->members.size();
+  int32_t done = 0;
+  while (done < nsteps) {
+    const int32_t chunk = std::min<int32_t>(nsteps - done, LCS_MAX_ASYNC_STEPS);
+    int first_rc = LCS_OK;
+    std::string first_err;
+    int32_t begun = 0;
+    for (; begun < m; begun++) {  // enqueue every member before waiting for any
+      const int rc = lcs_step_begin(b->members[begun], chunk);
+      if (rc != LCS_OK) {
+        first_rc = rc;
+        first_err = "batch member " + std::to_string(begun) + ": " + handle_error(b->members[begun]);
+        break;
+      }
+    }
+    for (int32_t i = 0; i < begun; i++) {
+      const int rc = lcs_step_finish(b->members[i], logs ? logs + (size_t)i * nsteps + done : nullptr);
+      if (rc != LCS_OK && first_rc == LCS_OK) {
+        first_rc = rc;
+        first_err = "batch member " + std::to_string(i) + ": " + handle_error(b->members[i]);
+      }
+    }
+    if (first_rc != LCS_OK) return serve_fail(first_rc, first_err);
+    done += chunk;
+  }
+  return LCS_OK;
+}
+
+void lcs_batch_destroy(lcs_batch* b) {
+  if (!b) return;
+  for (lcs_handle* h : b->members) lcs_destroy(h);
+  delete b;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------- server
+namespace {
+
+struct SpeciesData {
+  std::vector<int64_t> ids;
+  std::vector<double> diam, x, y, z, u, v, w;
+};
+
+struct Request {
+  int64_t ticket = 0;
+  lcs_config cfg{};
+  // inputs (released once the run is on the device)
+  std::vector<double> U, V, W, P;
+  std::vector<SpeciesData> sp;
+  int interp = 0;
+  int64_t nsteps = 0, steps_done = 0;
+  int64_t bytes = 0;
+  // scheduler-thread state
+  lcs_handle* h = nullptr;
+  int32_t in_flight = 0;
+  // outcome
+  int state = LCS_REQ_QUEUED;
+  int rc = LCS_OK;
+  std::string err;
+  std::vector<double> rU, rV, rW, rP;
+  std::vector<SpeciesData> rsp;
+  lcs_log last{};
+  Clock::time_point t_submit, t_done;
+};
+
+int64_t interior_cells(const lcs_config& c) { return (int64_t)c.dims[0] * c.dims[1] * c.dims[2]; }
+
+double percentile(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double pos = q * (double)(v.size() - 1);  // linear interpolation between order statistics
+  const size_t lo = (size_t)std::floor(pos), hi = std::min(lo + 1, v.size() - 1);
+  return v[lo] + (v[hi] - v[lo]) * (pos - (double)lo);
+}
+
+}  // namespace
+
+struct lcs_server {
+  lcs_server_config cfg{};
+  std::mutex mu;
+  std::condition_variable cv;  // wakes the scheduler (submissions, stop) and drain (completions)
+  std::deque<Request*> queue;
+  std::map<int64_t, std::unique_ptr<Request>> all;
+  std::vector<double> latencies;
+  int64_t next_ticket = 1, submitted = 0, completed = 0, failed = 0, active_count = 0;
+  int64_t bytes_in_use = 0, peak_bytes = 0;
+  double busy_s = 0.0;
+  bool stop = false;
+  std::thread th;
+  std::vector<Request*> active;  // scheduler thread only
+
+  // Create the run's handle and put its initial state on the device.
+  int start(Request* r) {
+    lcs_handle* h = nullptr;
+    int rc = lcs_create(&r->cfg, &h);
+    if (rc != LCS_OK) {
+      r->err = handle_error(nullptr);
+      return rc;
+    }
+    r->h = h;
+    rc = lcs_upload_flow(h, r->U.data(), r->V.data(), r->W.data(), r->P.data());
+    for (int s = 0; rc == LCS_OK && s < (int)r->sp.size(); s++) {
+      SpeciesData& d = r->sp[s];
+      rc = lcs_upload_particles(h, s, (int64_t)d.x.size(), d.ids.empty() ? nullptr : d.ids.data(), d.diam.data(),
+                                d.x.data(), d.y.data(), d.z.data(), d.u.data(), d.v.data(), d.w.data());
+      if (rc == LCS_OK && r->interp) rc = lcs_init_particle_velocity(h, s);
+    }
+    if (rc != LCS_OK) r->err = handle_error(h);
+    // the inputs are on the device now
+    std::vector<double>().swap(r->U);
+    std::vector<double>().swap(r->V);
+    std::vector<double>().swap(r->W);
+    std::vector<double>().swap(r->P);
+    std::vector<SpeciesData>().swap(r->sp);
+    return rc;
+  }
+
+  // Download the final state of a finished run and free its handle.
+  int finish(Request* r) {
+    const int64_t n3 = interior_cells(r->cfg);
+    r->rU.resize(n3);
+    r->rV.resize(n3);
+    r->rW.resize(n3);
+    r->rP.resize(n3);
+    int rc = lcs_download_flow(r->h, r->rU.data(), r->rV.data(), r->rW.data(), r->rP.data());
+    const int ns = r->cfg.mode == LCS_MODE_FLOW_PARTICLE ? r->cfg.n_species : 0;
+    r->rsp.resize(ns);
+    for (int s = 0; rc == LCS_OK && s < ns; s++) {
+      SpeciesData& d = r->rsp[s];
+      const size_t n = (size_t)r->cfg.species[s].nvalid;
+      d.ids.resize(n);
+      for (auto* a : {&d.diam, &d.x, &d.y, &d.z, &d.u, &d.v, &d.w}) a->resize(n);
+      rc = lcs_download_particles(r->h, s, d.ids.data(), d.diam.data(), d.x.data(), d.y.data(), d.z.data(),
+                                  d.u.data(), d.v.data(), d.w.data());
+    }
+    if (rc != LCS_OK) r->err = handle_error(r->h);
+    lcs_destroy(r->h);
+    r->h = nullptr;
+    return rc;
+  }
+
+  void retire(Request* r, int rc) {
+    std::lock_guard<std::mutex> lk(mu);
+    r->t_done = Clock::now();
+    bytes_in_use -= r->bytes;
+    active_count--;
+    if (rc == LCS_OK) {
+      r->state = LCS_REQ_DONE;
+      completed++;
+      latencies.push_back(std::chrono::duration<double>(r->t_done - r->t_submit).count());
+    } else {
+      r->state = LCS_REQ_FAILED;
+      r->rc = rc;
+      failed++;
+    }
+    cv.notify_all();
+  }
+
+  void run() {
+    std::vector<lcs_log> logs;
+    auto t_busy = Clock::now();
+    while (true) {
+      bool progressed = false;
+      // 1. admission: oldest first, while a slot is free and the budget holds
+      while (true) {
+        Request* r = nullptr;
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          if (stop) return;
+          if (queue.empty() || (int)active.size() >= cfg.max_active) break;
+          Request* q = queue.front();
+          if (bytes_in_use + q->bytes > cfg.hbm_budget_bytes) {
+            if (active.empty()) {  // it would not fit even alone
+              queue.pop_front();
+              q->state = LCS_REQ_FAILED;
+              q->rc = LCS_ENOMEM;
+              q->err = "request needs " + std::to_string(q->bytes) + " device bytes, over the server budget";
+              q->t_done = Clock::now();
+              failed++;
+              cv.notify_all();
+              continue;
+            }
+            break;
+          }
+          queue.pop_front();
+          bytes_in_use += q->bytes;
+          peak_bytes = std::max(peak_bytes, bytes_in_use);
+          if (active_count == 0) t_busy = Clock::now();
+          active_count++;
+          q->state = LCS_REQ_RUNNING;
+          r = q;
+        }
+        const int rc = start(r);
+        progressed = true;
+        if (rc != LCS_OK) {
+          if (r->h) lcs_destroy(r->h);
+          r->h = nullptr;
+          retire(r, rc);
+          continue;
+        }
+        active.push_back(r);
+      }
+      // 2. keep a slice of steps in flight for every admitted run
+      for (Request* r : active) {
+        if (r->in_flight || r->steps_done >= r->nsteps) continue;
+        const int32_t n = (int32_t)std::min<int64_t>(cfg.steps_per_slice, r->nsteps - r->steps_done);
+        const int rc = lcs_step_begin(r->h, n);
+        if (rc != LCS_OK) {
+          r->err = handle_error(r->h);
+          r->rc = rc;
+          r->steps_done = r->nsteps + 1;  // marks the failure for step 3
+          continue;
+        }
+        r->in_flight = n;
+      }
+      // 3. collect finished slices; retire finished runs
+      for (size_t i = 0; i < active.size();) {
+        Request* r = active[i];
+        bool finished = r->steps_done > r->nsteps;  // a failed begin
+        int rc = finished ? r->rc : LCS_OK;
+        if (!finished && r->in_flight) {
+          int32_t done = 0;
+          rc = lcs_step_poll(r->h, &done);
+          if (rc == LCS_OK && done) {
+            logs.resize(r->in_flight);
+            rc = lcs_step_finish(r->h, logs.data());
+            if (rc == LCS_OK) {
+              r->steps_done += r->in_flight;
+              r->last = logs.back();
+            }
+            r->in_flight = 0;
+            progressed = true;
+          }
+          if (rc != LCS_OK) {
+            r->err = handle_error(r->h);
+            finished = true;
+          }
+        }
+        if (!finished && r->steps_done >= r->nsteps && !r->in_flight) {
+          finished = true;
+          rc = finish(r);
+        }
+        if (finished) {
+          if (r->h) {
+            lcs_destroy(r->h);
+            r->h = nullptr;
+          }
+          {
+            std::lock_guard<std::mutex> lk(mu);
+            if (active_count == 1) busy_s += std::chrono::duration<double>(Clock::now() - t_busy).count();
+          }
+          retire(r, rc);
+          active.erase(active.begin() + (long)i);
+          progressed = true;
+          continue;
+        }
+        i++;
+      }
+      if (!progressed) {
+        std::unique_lock<std::mutex> lk(mu);
+        if (stop) return;
+        if (active.empty() && queue.empty()) {
+          cv.wait_for(lk, std::chrono::milliseconds(50));
+        } else {
+          lk.unlock();
+          std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+      }
+    }
+  }
+};
+
+extern "C" {
+
+int lcs_server_create(const lcs_server_config* c, lcs_server** out) {
+  if (!out) return serve_fail(LCS_EINVAL, "null output");
+  *out = nullptr;
+  if (!c) return serve_fail(LCS_EINVAL, "null server config");
+  if (c->max_active < 1) return serve_fail(LCS_EINVAL, "max_active must be >= 1");
+  if (c->steps_per_slice < 1 || c->steps_per_slice > LCS_MAX_ASYNC_STEPS)
+    return serve_fail(LCS_EINVAL, "steps_per_slice out of range");
+  if (c->hbm_budget_bytes <= 0) return serve_fail(LCS_EINVAL, "hbm_budget_bytes must be positive");
+  std::unique_ptr<lcs_server> s(new lcs_server);
+  s->cfg = *c;
+  s->th = std::thread([p = s.get()] { p->run(); });
+  *out = s.release();
+  return LCS_OK;
+}
+
+int lcs_server_submit(lcs_server* s, const lcs_request* r, int64_t* ticket) {
+  if (!s || !r || !ticket) return serve_fail(LCS_EINVAL, "null argument");
+  if (!r->U || !r->V || !r->W || !r->P) return serve_fail(LCS_EINVAL, "null initial field");
+  if (r->nsteps < 0) return serve_fail(LCS_EINVAL, "nsteps < 0");
+  std::unique_ptr<Request> q(new Request);
+  q->cfg = r->config;
+  q->cfg.use_graphs = 1;
+  q->cfg.device = s->cfg.device;
+  int64_t bytes = 0;
+  const int rc = lcs_footprint(&q->cfg, &bytes);  // validates the config too
+  if (rc != LCS_OK) return serve_fail(rc, handle_error(nullptr));
+  q->bytes = bytes;
+  const int64_t n3 = interior_cells(q->cfg);
+  q->U.assign(r->U, r->U + n3);
+  q->V.assign(r->V, r->V + n3);
+  q->W.assign(r->W, r->W + n3);
+  q->P.assign(r->P, r->P + n3);
+  const int ns = q->cfg.mode == LCS_MODE_FLOW_PARTICLE ? q->cfg.n_species : 0;
+  q->sp.resize(ns);
+  for (int sp = 0; sp < ns; sp++) {
+    const lcs_species_state& in = r->species[sp];
+    const size_t n = (size_t)q->cfg.species[sp].nvalid;
+    if (!in.diam || !in.x || !in.y || !in.z || !in.u || !in.v || !in.w)
+      return serve_fail(LCS_EINVAL, "null particle array in species " + std::to_string(sp));
+    SpeciesData& d = q->sp[sp];
+    if (in.ids) d.ids.assign(in.ids, in.ids + n);
+    d.diam.assign(in.diam, in.diam + n);
+    d.x.assign(in.x, in.x + n);
+    d.y.assign(in.y, in.y + n);
+    d.z.assign(in.z, in.z + n);
+    d.u.assign(in.u, in.u + n);
+    d.v.assign(in.v, in.v + n);
+    d.w.assign(in.w, in.w + n);
+  }
+  q->interp = r->interp_velocity;
+  q->nsteps = r->nsteps;
+  q->t_submit = Clock::now();
+  std::lock_guard<std::mutex> lk(s->mu);
+  q->ticket = s->next_ticket++;
+  *ticket = q->ticket;
+  s->queue.push_back(q.get());
+  s->all[q->ticket] = std::move(q);
+  s->submitted++;
+  s->cv.notify_all();
+  return LCS_OK;
+}
+
+int lcs_server_poll(lcs_server* s, int64_t ticket, int32_t* state, int64_t* steps_done) {
+  if (!s || !state) return serve_fail(LCS_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return serve_fail(LCS_EINVAL, "unknown ticket");
+  *state = it->second->state;
+  if (steps_done) *steps_done = std::min(it->second->steps_done, it->second->nsteps);
+  return LCS_OK;
+}
+
+int lcs_server_result(lcs_server* s, int64_t ticket, double* U, double* V, double* W, double* P,
+                      lcs_species_out* species, lcs_log* last_log, double* latency_s) {
+  if (!s) return serve_fail(LCS_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return serve_fail(LCS_EINVAL, "unknown ticket");
+  Request* r = it->second.get();
+  if (r->state == LCS_REQ_FAILED) return serve_fail(r->rc, r->err);
+  if (r->state != LCS_REQ_DONE) return serve_fail(LCS_ESTATE, "the request has not finished");
+  auto put = [](double* dst, const std::vector<double>& src) {
+    if (dst) std::memcpy(dst, src.data(), src.size() * sizeof(double));
+  };
+  put(U, r->rU);
+  put(V, r->rV);
+  put(W, r->rW);
+  put(P, r->rP);
+  if (species)
+    for (size_t sp = 0; sp < r->rsp.size(); sp++) {
+      const SpeciesData& d = r->rsp[sp];
+      put(species[sp].x, d.x);
+      put(species[sp].y, d.y);
+      put(species[sp].z, d.z);
+      put(species[sp].u, d.u);
+      put(species[sp].v, d.v);
+      put(species[sp].w, d.w);
+    }
+  if (last_log) *last_log = r->last;
+  if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+  return LCS_OK;
+}
+
+int lcs_server_release(lcs_server* s, int64_t ticket) {
+  if (!s) return serve_fail(LCS_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(ticket);
+  if (it == s->all.end()) return serve_fail(LCS_EINVAL, "unknown ticket");
+  const int st = it->second->state;
+  if (st != LCS_REQ_DONE && st != LCS_REQ_FAILED) return serve_fail(LCS_ESTATE, "the request has not finished");
+  s->all.erase(it);
+  return LCS_OK;
+}
+
+int lcs_server_stats_get(lcs_server* s, lcs_server_stats* out) {
+  if (!s || !out) return serve_fail(LCS_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  out->submitted = s->submitted;
+  out->completed = s->completed;
+  out->failed = s->failed;
+  out->queued = (int64_t)s->queue.size();
+  out->active = s->active_count;
+  out->bytes_in_use = s->bytes_in_use;
+  out->peak_bytes_in_use = s->peak_bytes;
+  out->p50_latency_s = percentile(s->latencies, 0.50);
+  out->p99_latency_s = percentile(s->latencies, 0.99);
+  double m = 0.0;
+  for (double v : s->latencies) m += v;
+  out->mean_latency_s = s->latencies.empty() ? 0.0 : m / (double)s->latencies.size();
+  out->busy_s = s->busy_s;
+  return LCS_OK;
+}
+
+int lcs_server_drain(lcs_server* s, double timeout_s) {
+  if (!s) return serve_fail(LCS_EINVAL, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  const auto until = Clock::now() + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(timeout_s));
+  while (s->completed + s->failed < s->submitted) {
+    if (s->cv.wait_until(lk, until) == std::cv_status::timeout && s->completed + s->failed < s->submitted)
+      return serve_fail(LCS_ETIMEDOUT, "requests still running after the drain timeout");
+  }
+  return LCS_OK;
+}
+
+void lcs_server_destroy(lcs_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    s->cv.notify_all();
+  }
+  if (s->th.joinable()) s->th.join();
+  for (Request* r : s->active) {
+    if (r->h) {
+      if (r->in_flight) lcs_step_finish(r->h, nullptr);  // let in-flight work end before freeing its memory
+      lcs_destroy(r->h);
+    }
+  }
+  delete s;
+}
+
+}  // extern "C"

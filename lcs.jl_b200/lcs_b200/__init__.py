@@ -9,7 +9,8 @@ library liblcs_b200.so; this package only prepares inputs and reads results.
 from . import _abi, config, inits
 from .config import RunConfig, from_dict, readconfig, workload
 from .engine import Engine, LCSError, footprint
+from .serve import Batch, Server
 from .simulate import init_engine, simulate
 
-__all__ = ["Engine", "LCSError", "RunConfig", "_abi", "config", "footprint", "from_dict", "init_engine", "inits",
+__all__ = ["Batch", "Server", "Engine", "LCSError", "RunConfig", "_abi", "config", "footprint", "from_dict", "init_engine", "inits",
            "readconfig", "simulate", "workload"]

@@ -118,6 +118,40 @@ _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 _I64 = C.POINTER(C.c_int64)
 
+
+# ---- batching and serving forms (include/lcs_b200.h) -----------------------
+MAX_ASYNC_STEPS = 4096
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_active", C.c_int32), ("steps_per_slice", C.c_int32), ("_pad", C.c_int32),
+                ("hbm_budget_bytes", C.c_int64)]
+
+
+class SpeciesState(C.Structure):
+    _fields_ = [("ids", _I64), ("diam", _D), ("x", _D), ("y", _D), ("z", _D), ("u", _D), ("v", _D), ("w", _D)]
+
+
+class Request(C.Structure):
+    _fields_ = [("config", Config), ("U", _D), ("V", _D), ("W", _D), ("P", _D),
+                ("species", SpeciesState * MAX_SPECIES), ("interp_velocity", C.c_int32), ("_pad", C.c_int32),
+                ("nsteps", C.c_int64)]
+
+
+class SpeciesOut(C.Structure):
+    _fields_ = [("x", _D), ("y", _D), ("z", _D), ("u", _D), ("v", _D), ("w", _D)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("queued", C.c_int64),
+                ("active", C.c_int64), ("bytes_in_use", C.c_int64), ("peak_bytes_in_use", C.c_int64),
+                ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double), ("mean_latency_s", C.c_double),
+                ("busy_s", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
 # name -> (restype, argtypes) for every entry point of include/lcs_b200.h
 PROTOTYPES = {
     "lcs_create": (C.c_int, [C.POINTER(Config), C.POINTER(_P)]),
@@ -159,6 +193,24 @@ PROTOTYPES = {
     "lcs_synchronize": (C.c_int, [_P]),
     "lcs_flow_timestep_noalloc": (C.c_int, [_P, _P, _P, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_double,
                                             C.c_double, _P, _P]),
+    "lcs_step_begin": (C.c_int, [_P, C.c_int32]),
+    "lcs_step_poll": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "lcs_step_finish": (C.c_int, [_P, C.POINTER(Log)]),
+    "lcs_device_bytes": (C.c_int, [_P, _I64]),
+    "lcs_batch_create": (C.c_int, [C.POINTER(Config), C.c_int32, C.POINTER(_P)]),
+    "lcs_batch_size": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "lcs_batch_member": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
+    "lcs_batch_step": (C.c_int, [_P, C.c_int32, C.POINTER(Log)]),
+    "lcs_batch_destroy": (None, [_P]),
+    "lcs_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_P)]),
+    "lcs_server_submit": (C.c_int, [_P, C.POINTER(Request), _I64]),
+    "lcs_server_poll": (C.c_int, [_P, C.c_int64, C.POINTER(C.c_int32), _I64]),
+    "lcs_server_result": (C.c_int, [_P, C.c_int64, _D, _D, _D, _D, C.POINTER(SpeciesOut), C.POINTER(Log), _D]),
+    "lcs_server_release": (C.c_int, [_P, C.c_int64]),
+    "lcs_server_stats_get": (C.c_int, [_P, C.POINTER(ServerStats)]),
+    "lcs_server_drain": (C.c_int, [_P, C.c_double]),
+    "lcs_server_destroy": (None, [_P]),
+    "lcs_serve_last_error": (C.c_char_p, []),
 }
 
 NOALLOC_MAX_PLANES = 4096

@@ -49,10 +49,23 @@ class Engine:
             raise LCSError(rc, self.lib.lcs_last_error(None).decode())
         self.handle = h
 
+    @classmethod
+    def borrow(cls, lib, cfg: _abi.Config, handle) -> "Engine":
+        """A view of a handle owned elsewhere (a batch member): every method
+        works, and close() leaves the handle to its owner."""
+        e = cls.__new__(cls)
+        e.lib, e.cfg = lib, cfg
+        e.n = tuple(int(d) for d in cfg.dims)
+        e.h = int(cfg.halo_size)
+        e.handle = handle
+        e._borrowed = True
+        return e
+
     # -- lifetime ----------------------------------------------------------
     def close(self):
         if getattr(self, "handle", None):
-            self.lib.lcs_destroy(self.handle)
+            if not getattr(self, "_borrowed", False):
+                self.lib.lcs_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

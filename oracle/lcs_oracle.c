@@ -63,6 +63,9 @@ struct lcs_handle {
   species_t sp[LCS_MAX_SPECIES];
   int64_t step;
   double t;
+  int32_t async_n;                 /* steps of a pending lcs_step_begin (run at begin) */
+  int32_t async_rc;
+  lcs_log* async_logs;
   char err[512];
 };
 
@@ -898,6 +901,7 @@ void lcs_destroy(lcs_handle* h) {
     for (int q = 0; q < LCS_NPROP; q++) free(h->sp[s].p[q]);
     free(h->sp[s].ids);
   }
+  free(h->async_logs);
   free(h);
 }
 
@@ -1065,6 +1069,39 @@ int lcs_step_timed(lcs_handle* h, int32_t nsteps, lcs_log* logs, double* ms) {
   if (ms) *ms = (omp_get_wtime() - t0) * 1e3;
   return rc;
 }
+/* Asynchronous steps on the CPU: the steps run inside lcs_step_begin, poll
+ * reports them done, finish returns their logs. */
+int lcs_step_begin(lcs_handle* h, int32_t nsteps) {
+  if (!h) return LCS_EINVAL;
+  if (h->async_n) return fail(h, LCS_ESTATE, "steps are already in flight on this handle");
+  if (nsteps < 1 || nsteps > LCS_MAX_ASYNC_STEPS) return fail(h, LCS_EINVAL, "nsteps must be in 1..%d", LCS_MAX_ASYNC_STEPS);
+  free(h->async_logs);
+  h->async_logs = (lcs_log*)calloc((size_t)nsteps, sizeof(lcs_log));
+  if (!h->async_logs) return fail(h, LCS_ENOMEM, "host allocation failed");
+  h->async_rc = lcs_step(h, nsteps, h->async_logs);
+  h->async_n = nsteps;
+  return LCS_OK;
+}
+int lcs_step_poll(lcs_handle* h, int32_t* done) {
+  if (!h || !done) return LCS_EINVAL;
+  if (!h->async_n) return fail(h, LCS_ESTATE, "no steps in flight on this handle");
+  *done = 1;
+  return LCS_OK;
+}
+int lcs_step_finish(lcs_handle* h, lcs_log* logs) {
+  if (!h) return LCS_EINVAL;
+  if (!h->async_n) return fail(h, LCS_ESTATE, "no steps in flight on this handle");
+  const int32_t n = h->async_n;
+  h->async_n = 0;
+  if (h->async_rc) return h->async_rc;
+  if (logs) memcpy(logs, h->async_logs, (size_t)n * sizeof(lcs_log));
+  return LCS_OK;
+}
+int lcs_device_bytes(lcs_handle* h, int64_t* bytes) {
+  if (!h || !bytes) return LCS_EINVAL;
+  return lcs_footprint(&h->cfg, bytes);
+}
+
 int lcs_transfer_stats(lcs_handle* h, int64_t* a, int64_t* b) {
   if (!h) return LCS_EINVAL;
   if (a) *a = 0;

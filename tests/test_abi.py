@@ -70,6 +70,26 @@ def test_struct_layout_matches_c():
     assert offs == cfg_offs + log_offs
 
 
+@pytest.mark.parametrize("cname,pyname", [("lcs_server_config", "ServerConfig"), ("lcs_species_state", "SpeciesState"),
+                                          ("lcs_request", "Request"), ("lcs_species_out", "SpeciesOut"),
+                                          ("lcs_server_stats", "ServerStats")])
+def test_serving_struct_layouts_match_c(cname, pyname):
+    st = getattr(_abi, pyname)
+    fields = [f for f, _ in st._fields_]
+    prog = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {",
+            f'printf("%zu\\n", sizeof({cname}));']
+    prog += [f'printf("%zu\\n", offsetof({cname}, {f}));' for f in fields]
+    prog.append("return 0; }")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.c")
+        open(src, "w").write("\n".join(prog))
+        exe = os.path.join(d, "t")
+        subprocess.run(["/usr/bin/gcc", src, "-o", exe], check=True)
+        vals = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
+    assert vals[0] == C.sizeof(st)
+    assert vals[1:] == [getattr(st, f).offset for f in fields]
+
+
 def test_footprint_and_validation_without_gpu(cuda_lib_path):
     lib = _abi.bind(C.CDLL(cuda_lib_path))
     b = C.c_int64()

@@ -43,17 +43,21 @@ from lcs_b200 import config as lcfg  # noqa: E402
 from lcs_b200 import inits  # noqa: E402
 
 WORKLOADS = {
-    # the plain FP64 method at 256^3 with rc-energy forcing
+    # the plain FP64 method at 256^3 with rc-energy forcing (the default bench workload)
     "rc256": dict(n=256, nu=0.005, forcing={"kind": "rc-energy", "params": {"kmin": 1, "kmax": 2, "energy": 0.649,
                                                                             "coarse_size": 16}},
                   taups=[0.05, 0.5], counts=[2 ** 19, 2 ** 19], precision="fp64"),
-    # 128^3, linear-power P = 0.5, 65,536 particles tau_p = 0.1
+    # the CPU-runnable case: 128^3, linear-power P = 0.5, 65,536 particles tau_p = 0.1
     "lp128": dict(n=128, nu=0.01, forcing={"kind": "linear-power", "params": {"power": 0.5}}, taups=[0.1],
                   counts=[65536], precision="fp64"),
-    # configs[2] at FP64 (the FP32-mixed form is not built yet)
+    # the precision-form workload: 512^3, linear-power, 2^24 particles in 3 species
+    # (--precision selects the form; --report precision compares both)
     "lp512": dict(n=512, nu=0.0025, forcing={"kind": "linear-power", "params": {"power": 0.5}},
                   taups=[0.02, 0.2, 2.0], counts=[2 ** 24 // 3, 2 ** 24 // 3, 2 ** 24 - 2 * (2 ** 24 // 3)],
                   precision="fp64"),
+    # the 64-member ensemble and the served request stream: run_batch and run_serve
+    "batch64": None,
+    "serve": None,
 }
 
 # DRAM bytes (read + write) per launch of the sweep kernel, per interior cell:
@@ -385,6 +389,211 @@ def run_b200(args):
     return 0
 
 
+# ---------------------------------------------------------------- precision report
+def run_precision_report(args):
+    """The precision-form workload: the FP32-mixed form against the plain FP64 form
+    on the same workload and seed after --steps steps: throughput of both, and
+    the FP32-mixed error per field (rel-L2 of U, V, W, P), per flow statistic
+    (urms, epsilon, Re_lambda, skewness of the restated Flows.stat), per E(k)
+    shell, and per particle species (rms velocity)."""
+    from lcs_b200 import Engine, stats
+
+    res = {}
+    for prec in ("fp64", "fp32-mixed"):
+        rc, w = make_run_config(args.workload, seed=0, precision=prec)
+        rc.abi.use_graphs = 1
+        flow, parts = host_inputs(rc)
+        eng = Engine(rc.abi)
+        load_engine(eng, rc, flow, parts)
+        eng.step(1)  # warm-up (graph build), then the timed steps
+        eng.synchronize()
+        logs, ms = eng.step_timed(args.steps)
+        n3 = float(np.prod(rc.dims))
+        out_flow = eng.download_flow()
+        out_parts = [eng.download_particles(s) for s in range(len(parts))]
+        eng.close()
+        st = stats.flow_stat(*out_flow[:3], nu=w["nu"])
+        res[prec] = {"value": n3 * args.steps / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps,
+                     "sweeps_per_step": float(np.mean([lg["couple1"]["sweeps"] + lg["couple2"]["sweeps"] for lg in logs])),
+                     "flow": out_flow, "parts": out_parts, "stat": st,
+                     "spectrum": stats.energy_spectrum(*out_flow[:3])}
+    a, b = res["fp32-mixed"], res["fp64"]
+
+    def rel(x, y):
+        return float(abs(x - y) / abs(y)) if y != 0 else float(abs(x - y))
+
+    def rel_l2(x, y):
+        return float(np.linalg.norm((x - y).ravel()) / np.linalg.norm(y.ravel()))
+
+    ek_b, ek_a = b["spectrum"], a["spectrum"]
+    shells = [k for k in range(1, len(ek_b)) if ek_b[k] > 1e-12 * ek_b[1:].max()]
+    line = {
+        "metric": "Mcell-steps/s, FP32-mixed vs FP64", "workload": args.workload, "steps": args.steps,
+        "n": int(make_run_config(args.workload)[0].dims[0]),
+        "fp64": {k: b[k] for k in ("value", "ms_per_step", "sweeps_per_step")},
+        "fp32_mixed": {k: a[k] for k in ("value", "ms_per_step", "sweeps_per_step")},
+        "fp32_mixed_vs_fp64": a["value"] / b["value"],
+        "hsmac_epsp": "epsp = 1e-8 * dxmin in both forms (RMS div < 1e-8); neither reaches it, both run itrmax = 300",
+        "errors": {
+            "field_rel_l2": {f: rel_l2(x, y) for f, x, y in zip("UVWP", a["flow"], b["flow"])},
+            "stat_rel": {k: rel(a["stat"][k], b["stat"][k]) for k in ("urms", "k", "epsilon", "Re_lambda",
+                                                                     "skewness", "flatness")},
+            "spectrum_max_rel": max(rel(ek_a[k], ek_b[k]) for k in shells),
+            "spectrum_shells": len(shells),
+            "particle_rms_velocity_rel": [
+                rel(stats.particle_rms_velocity(pa["u"], pa["v"], pa["w"]),
+                    stats.particle_rms_velocity(pb["u"], pb["v"], pb["w"]))
+                for pa, pb in zip(a["parts"], b["parts"])],
+            "particle_position_rel_l2": [
+                float(np.sqrt(sum(np.sum((pa[k] - pb[k]) ** 2) for k in "xyz") / sum(np.sum(pb[k] ** 2) for k in "xyz")))
+                for pa, pb in zip(a["parts"], b["parts"])],
+        },
+        "fp64_stat": {k: b["stat"][k] for k in ("urms", "epsilon", "Re_lambda", "skewness", "flatness")},
+        "data": "synthetic (seeded spectral field, uniform random particles)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- batching form
+def ensemble_members(seed=0):
+    """The 64-member ensemble: 16 x 32^3, 24 x 48^3, 16 x 64^3, 8 x 96^3 with
+    per-member seeds, nu log-uniform in [0.01, 0.05], one species of 8k-128k
+    particles with tau_p log-uniform in [0.01, 1], linear-power forcing
+    P = 0.5, FP32-mixed."""
+    rng = np.random.default_rng(seed)
+    sizes = [32] * 16 + [48] * 24 + [64] * 16 + [96] * 8
+    members = []
+    for i, n in enumerate(sizes):
+        nu = float(np.exp(rng.uniform(np.log(0.01), np.log(0.05))))
+        taup = float(np.exp(rng.uniform(np.log(0.01), np.log(1.0))))
+        count = int(np.exp(rng.uniform(np.log(8192), np.log(131072))))
+        d = lcfg.workload(n, nu, {"kind": "linear-power", "params": {"power": 0.5}}, [taup], [count], seed=1000 + i,
+                          precision="fp32-mixed")
+        members.append(lcfg.from_dict(d))
+    return members
+
+
+def run_batch(args):
+    """The batching form: all 64 members stepped together (lcs_batch_step),
+    against the same members stepped one after another."""
+    from lcs_b200 import Batch, Engine
+
+    members = ensemble_members()
+    for rc in members:
+        rc.abi.use_graphs = 1
+    cells = float(sum(np.prod(rc.dims) for rc in members))
+    parts_total = float(sum(sum(si.nvalid for si in rc.species) for rc in members))
+    t_create = time.perf_counter()
+    b = Batch([rc.abi for rc in members])
+    create_s = time.perf_counter() - t_create
+    shapes = {}
+    for i, rc in enumerate(members):
+        shapes.setdefault(f"{rc.dims[0]}^3", b.tuning(i))
+    for rc, e in zip(members, b.members):
+        load_engine(e, rc, *host_inputs(rc))
+    b.step(max(1, args.warmup))
+    import ctypes as C
+
+    t0 = time.perf_counter()
+    logs = b.step(args.steps)
+    batch_s = time.perf_counter() - t0
+    sweeps = float(np.mean([lg["couple1"]["sweeps"] + lg["couple2"]["sweeps"] for ml in logs for lg in ml]))
+    launches = 0
+    for e in b.members:
+        n = C.c_int64()
+        e._check(e.lib.lcs_launch_count(e.handle, C.byref(n)))
+        launches += n.value
+    b.close()
+    # the same members one at a time (each on its own handle)
+    seq_steps = max(1, min(args.steps, 3))
+    seq_s = 0.0
+    for rc in members:
+        e = Engine(rc.abi)
+        load_engine(e, rc, *host_inputs(rc))
+        e.step(1)
+        e.synchronize()
+        t0 = time.perf_counter()
+        e.step(seq_steps)
+        seq_s += time.perf_counter() - t0
+        e.close()
+    value = cells * args.steps / batch_s / 1e6
+    seq_value = cells * seq_steps / seq_s / 1e6
+    print(json.dumps({
+        "metric": "Mcell-steps/s", "value": value, "unit": "Mcell-steps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": batch_s * 1e3 / args.steps, "higher_is_better": True,
+        "dtype": "f32 (FP64 residuals, reductions, positions)", "data": "synthetic (seeded spectral fields)",
+        "config": {"workload": "batch64", "members": len(members), "sizes": "16x32^3, 24x48^3, 16x64^3, 8x96^3",
+                   "cells": int(cells), "particles": int(parts_total), "precision": "fp32-mixed"},
+        "particle_steps_per_s": parts_total * args.steps / batch_s,
+        "hsmac_sweeps_per_member_step": sweeps,
+        "sequential": {"value": seq_value, "steps": seq_steps, "note": "the members one after another, each alone"},
+        "batch_vs_sequential": value / seq_value,
+        "autotune": {"create_s": create_s, "chosen": shapes},
+        "timing": "host wall clock around lcs_batch_step (all members enqueued, then all waited for)",
+    }), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ serving form
+def run_serve(args):
+    """The serving form: a seeded Poisson stream (--rate per second) of
+    --requests requests with N in {32, 48, 64, 96, 128, 192}, 10^4-10^6
+    particles with tau_p log-uniform in [0.01, 2], 50-500 steps (times
+    --steps-scale), FP32-mixed, admitted under a 150 GB budget."""
+    from lcs_b200 import Server, _abi
+
+    rng = np.random.default_rng(2026)
+    sizes = [32, 48, 64, 96, 128, 192]
+    flows = {}
+    for n in sizes:  # one seeded spectral field per size (the inputs are not timed)
+        flows[n] = inits.spectral_flow(n, seed=n)
+    srv = Server(device=int(os.environ.get("LCS_DEVICE", "0")), max_active=int(os.environ.get("LCS_SERVE_SLOTS", "32")),
+                 steps_per_slice=4, hbm_budget_bytes=150 * 10 ** 9)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
+    tickets, work = [], 0.0
+    t0 = time.perf_counter()
+    for r in range(args.requests):
+        n = int(rng.choice(sizes))
+        count = int(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
+        taup = float(np.exp(rng.uniform(np.log(0.01), np.log(2.0))))
+        steps = max(1, int(round(rng.integers(50, 501) * args.steps_scale)))
+        d = lcfg.workload(n, 0.01, {"kind": "linear-power", "params": {"power": 0.5}}, [taup], [count], seed=r,
+                          precision="fp32-mixed")
+        rc = lcfg.from_dict(d)
+        x, y, z = inits.random_positions(count, 7 + r)
+        zero = np.zeros(count)
+        sp = [{"diam": np.full(count, rc.species[0].diam), "x": x, "y": y, "z": z, "u": zero, "v": zero, "w": zero}]
+        delay = arrivals[r] - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        tickets.append(srv.submit(rc.abi, *flows[n], species=sp, nsteps=steps, interp_velocity=True))
+        work += float(n) ** 3 * steps
+    srv.drain(timeout_s=float(os.environ.get("LCS_SERVE_TIMEOUT_S", "3600")))
+    makespan = time.perf_counter() - t0
+    st = srv.stats()
+    lat = []
+    for t in tickets:
+        state, _ = srv.poll(t)
+        if state == _abi.REQ_DONE:
+            lat.append(srv.result(t)["latency_s"])
+        srv.release(t)
+    srv.close()
+    print(json.dumps({
+        "metric": "served solves/s; p50/p99 time-to-completion", "value": st["completed"] / makespan,
+        "unit": "solves/s", "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+        "mean_latency_s": st["mean_latency_s"], "completed": st["completed"], "failed": st["failed"],
+        "makespan_s": makespan, "Mcell_steps_per_s": work / makespan / 1e6,
+        "peak_bytes_in_use": st["peak_bytes_in_use"], "busy_s": st["busy_s"],
+        "config": {"workload": "serve", "requests": args.requests, "rate_per_s": args.rate,
+                   "steps_scale": args.steps_scale, "sizes": sizes, "hbm_budget_bytes": 150 * 10 ** 9,
+                   "slots": int(os.environ.get("LCS_SERVE_SLOTS", "32")), "precision": "fp32-mixed"},
+        "data": "synthetic (one seeded spectral field per size, seeded particles and request stream)",
+        "timing": "host wall clock; latency = submit to result ready",
+    }), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,9 +604,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "fp32-mixed"], default="fp64")
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other precision form")
+    ap.add_argument("--report", choices=["precision"], default=None,
+                    help="precision: FP32-mixed vs FP64 errors per field and statistic (config 2)")
+    ap.add_argument("--requests", type=int, default=1000, help="serve: number of requests")
+    ap.add_argument("--steps-scale", type=float, default=1.0, help="serve: scale of the 50-500 step counts")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: mean arrivals per second")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.report == "precision":
+        return run_precision_report(args)
+    if args.workload == "batch64":
+        return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_b200(args)
 
 

@@ -236,6 +236,13 @@ LCS_API int lcs_step_poll(lcs_handle* h, int32_t* done);
 LCS_API int lcs_step_finish(lcs_handle* h, lcs_log* logs);
 /* Device bytes the handle holds (its pool), as lcs_footprint predicts. */
 LCS_API int lcs_device_bytes(lcs_handle* h, int64_t* bytes);
+/* Launch shapes of a handle, set from outside (no reference counterpart; the
+ * batch's autotuner and the server use it): rw_rows = tile rows of the
+ * HSMAC sweep (13, 8 or 5; 0 keeps the current), zchunk = planes per z chunk
+ * of a sweep (0: the built-in cost model), share = the part of the GPU the
+ * handle's launches are sized for when several handles run at once (0, 1].
+ * Results do not depend on these; the step graphs are captured again. */
+LCS_API int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, double share);
 
 /* ---- batching form (no reference counterpart) ---------------------------
  * An ensemble of independent runs with uneven grid sizes, particle counts and
@@ -250,6 +257,12 @@ LCS_API int lcs_batch_create(const lcs_config* members, int32_t m, lcs_batch** o
 LCS_API int lcs_batch_size(const lcs_batch* b, int32_t* m);
 LCS_API int lcs_batch_member(lcs_batch* b, int32_t i, lcs_handle** h);
 LCS_API int lcs_batch_step(lcs_batch* b, int32_t nsteps, lcs_log* logs);
+/* The launch shapes lcs_batch_create chose for member i (see lcs_set_tuning):
+ * its autotuner steps probe handles of each member shape together for every
+ * candidate tile height and z chunk and keeps the fastest (probe_ms, one
+ * probe step); LCS_BATCH_TUNE=0 in the environment skips the probing. */
+LCS_API int lcs_batch_tuning(const lcs_batch* b, int32_t i, int32_t* rw_rows, int32_t* zchunk, double* share,
+                             double* probe_ms);
 LCS_API void lcs_batch_destroy(lcs_batch* b);
 
 /* ---- serving form (no reference counterpart) ----------------------------

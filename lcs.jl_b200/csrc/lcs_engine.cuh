@@ -331,6 +331,7 @@ class Engine : public EngineBase {
       if (tma_ctas_per_sm < 1) return fail(LCS_ECUDA, "the TMA sweep does not fit on an SM");
     }
     LCS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, cfg.device));
+    encode_fn = encode;
     if (use_rw) {
       // row-warp sweep tile rows: LCS_B200_RW=13 (default: one CTA of 16 warps
       // per SM, fastest in both precisions) | 8 | 5
@@ -339,35 +340,45 @@ class Engine : public EngineBase {
         const std::string t(v);
         rw_variant = t == "8" ? 1 : t == "5" ? 2 : 0;
       }
-      switch (rw_variant) {
-        case 1: RTY = 8; rw_smem = RwLayout<T, 8, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 8, 3>;
-                rw_threads = RwLayout<T, 8, 3>::NT; break;
-        case 2: RTY = 5; rw_smem = RwLayout<T, 5, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 5, 3>;
-                rw_threads = RwLayout<T, 5, 3>::NT; break;
-        default: RTY = 13; rw_smem = RwLayout<T, 13, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 13, 3>;
-                 rw_threads = RwLayout<T, 13, 3>::NT; break;
-      }
-      const cuuint32_t rbox[3] = {(cuuint32_t)RW_W, (cuuint32_t)RTY + 4, 1};
-      for (int b = 0; b < kVelMaps; b++) {
-        CUresult rr = encode(&tmaps_rw.vel[b], dtype, 3, vel0[b / 3][b % 3], dims, strides,
-                             rbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (rr != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp velocity %d) failed: %d", b,
-                                            (int)rr);
-      }
-      const cuuint32_t rpbox[3] = {(cuuint32_t)RW_W, (cuuint32_t)RTY, 1};
-      CUresult rp = encode(&tmaps_rw.P, dtype, 3, (void*)P, dims, strides, rpbox, estr,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (rp != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp P) failed: %d", (int)rp);
-      LCS_CUDA(cudaFuncSetAttribute(rw_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
-    }
-    if (use_rw) {
-      LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rw_ctas_per_sm, rw_fn, rw_threads, rw_smem));
-      if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the row-warp sweep does not fit on an SM");
+      LCS_TRY(init_rw_maps());
     }
     return LCS_OK;
   }
+  // The row-warp sweep of the current rw_variant: kernel, shared memory,
+  // occupancy and its tensor maps (box 64 x rows+4 and 64 x rows).
+  int init_rw_maps() {
+    switch (rw_variant) {
+      case 1: RTY = 8; rw_smem = RwLayout<T, 8, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 8, 3>;
+              rw_threads = RwLayout<T, 8, 3>::NT; break;
+      case 2: RTY = 5; rw_smem = RwLayout<T, 5, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 5, 3>;
+              rw_threads = RwLayout<T, 5, 3>::NT; break;
+      default: RTY = 13; rw_smem = RwLayout<T, 13, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 13, 3>;
+               rw_threads = RwLayout<T, 13, 3>::NT; break;
+    }
+    const CUtensorMapDataType dtype =
+        std::is_same<T, double>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)(g.n[1] + 2 * g.h), (cuuint64_t)(g.n[2] + 2 * g.h)};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.pz * sizeof(T)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const cuuint32_t rbox[3] = {(cuuint32_t)RW_W, (cuuint32_t)RTY + 4, 1};
+    for (int b = 0; b < kVelMaps; b++) {
+      CUresult rr = encode_fn(&tmaps_rw.vel[b], dtype, 3, vel0[b / 3][b % 3], dims, strides, rbox, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (rr != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp velocity %d) failed: %d", b,
+                                          (int)rr);
+    }
+    const cuuint32_t rpbox[3] = {(cuuint32_t)RW_W, (cuuint32_t)RTY, 1};
+    CUresult rp = encode_fn(&tmaps_rw.P, dtype, 3, (void*)P, dims, strides, rpbox, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (rp != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp P) failed: %d", (int)rp);
+    LCS_CUDA(cudaFuncSetAttribute(rw_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
+    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rw_ctas_per_sm, rw_fn, rw_threads, rw_smem));
+    if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the row-warp sweep does not fit on an SM");
+    return LCS_OK;
+  }
+  PFN_cuTensorMapEncodeTiled_v12000 encode_fn = nullptr;
   int num_sms = 148, tma_ctas_per_sm = 1;
   bool use_rw = false;
   TensorMaps tmaps_rw;
@@ -572,7 +583,13 @@ class Engine : public EngineBase {
   // one pass over tiles whose first column is odd (16-byte TMA rule)
   // z chunk of a TMA-fed sweep: minimise (waves of resident CTAs) x (planes
   // per chunk + the 4 warm-up/drain planes a chunk costs)
+  // Share of the GPU this handle's launches are sized for: 1 alone; a batch
+  // member or served run gets its part, so that concurrent runs do not each
+  // split their work to fill every SM.
+  double sm_share = 1.0;
+  int share_slots(int slots) const { return std::max(1, (int)std::lround(slots * sm_share)); }
   int pick_zchunk(int nzc, int ncols, int slots) const {
+    slots = share_slots(slots);
     int best_nc = 1;
     double best = 1e300;
     for (int nc = 1; nc <= std::min(nzc, 64); nc++) {
@@ -691,11 +708,15 @@ class Engine : public EngineBase {
     int64_t slab_cells = 0;  // the face kernel indexes a pair of slabs with 32-bit integers
     for (int q = 0; q < 6; q++)
       slab_cells = std::max<int64_t>(slab_cells, (int64_t)((f[q].len(0) + 1) / 2) * f[q].len(1) * f[q].len(2));
+    // blocks: enough for one round of the largest phase (4 cells per thread),
+    // at most the co-resident grid and the handle's share of it
+    const int fblocks = (int)std::max<int64_t>(
+        1, std::min<int64_t>({(int64_t)face_grid, (int64_t)share_slots(face_grid), (2 * slab_cells + 1023) / 1024}));
     if (face_grid > 0 && core_nonempty && cfg.coloring != LCS_COLORING_RED_BLACK_BLOCK &&
-        used + face_grid <= plan.partials_cap && 2 * slab_cells < INT32_MAX) {
+        used + fblocks <= plan.partials_cap && 2 * slab_cells < INT32_MAX) {
       FaceSet fs;
       for (int q = 0; q < 6; q++) fs.f[q] = f[q];
-      return launch_coop("hsmac_faces", k_hsmac_faces<T>, dim3(face_grid), dim3(256), dctx, g, set, P, fs, hc,
+      return launch_coop("hsmac_faces", k_hsmac_faces<T>, dim3(fblocks), dim3(256), dctx, g, set, P, fs, hc,
                          partials, used, group_end);
     }
     for (int q = 0; q < 6; q++) LCS_TRY(phases(set, f[q], partials, &used));
@@ -1106,6 +1127,37 @@ class Engine : public EngineBase {
     return LCS_OK;
   }
   int64_t device_bytes() const override { return (int64_t)plan.bytes; }
+
+  // Launch shapes chosen from outside (the batch's autotuner, the server):
+  // rw_rows = tile rows of the row-warp sweep (13, 8 or 5; 0 keeps it),
+  // zchunk = planes per z chunk of the TMA sweeps (0: the cost model),
+  // share = part of the GPU the launches are sized for (0 < share <= 1).
+  // The step graphs are captured again with the new shapes.
+  int set_tuning(int rw_rows, int zchunk, double share) override {
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    if (rw_rows != 0 && rw_rows != 13 && rw_rows != 8 && rw_rows != 5) return fail(LCS_EINVAL, "rw_rows must be 0, 13, 8 or 5");
+    if (zchunk < 0) return fail(LCS_EINVAL, "zchunk < 0");
+    if (!(share > 0.0 && share <= 1.0)) return fail(LCS_EINVAL, "share must be in (0, 1]");
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    if (rw_rows != 0 && use_rw) {
+      rw_variant = rw_rows == 8 ? 1 : rw_rows == 5 ? 2 : 0;
+      LCS_TRY(init_rw_maps());
+    }
+    zchunk_force = zchunk;
+    sm_share = share;
+    drop_graphs();
+    return LCS_OK;
+  }
+  void drop_graphs() {
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (step_graph) cudaGraphDestroy(step_graph);
+    if (evolve_exec) cudaGraphExecDestroy(evolve_exec);
+    if (evolve_graph) cudaGraphDestroy(evolve_graph);
+    step_exec = nullptr;
+    step_graph = nullptr;
+    evolve_exec = nullptr;
+    evolve_graph = nullptr;
+  }
 
   // Asynchronous steps (the batch and the server drive many handles at once):
   // step_begin enqueues nsteps graph replays of the step, then copies of the

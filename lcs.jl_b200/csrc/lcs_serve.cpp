@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -46,9 +47,114 @@ using Clock = std::chrono::steady_clock;
 }  // namespace
 
 // ------------------------------------------------------------------ batch
+struct MemberTuning {
+  int32_t rw_rows = 0, zchunk = 0;
+  double share = 1.0, probe_ms = 0.0;
+};
+
 struct lcs_batch {
   std::vector<lcs_handle*> members;
+  std::vector<lcs_config> cfgs;
+  std::vector<MemberTuning> tuning;
 };
+
+namespace {
+
+// The batch's autotuner.  Members that share a shape (dims and precision) get
+// the same launch shapes: for every candidate (tile rows of the sweep x z
+// chunk) it steps probe handles of that shape, one per member, together (zero
+// fields, exactly 20 sweeps per couple, no particles) and times one step; the
+// fastest candidate is applied to the members.  Probes never touch a member's
+// state, and no result depends on the launch shapes.
+int autotune(lcs_batch* b) {
+  const size_t m = b->members.size();
+  double total_cells = 0.0;
+  for (const auto& c : b->cfgs) total_cells += (double)c.dims[0] * c.dims[1] * c.dims[2];
+  std::vector<bool> done(m, false);
+  for (size_t i = 0; i < m; i++) {
+    if (done[i]) continue;
+    const lcs_config& ci = b->cfgs[i];
+    std::vector<size_t> group;
+    for (size_t q = i; q < m; q++) {
+      const lcs_config& cq = b->cfgs[q];
+      if (cq.dims[0] == ci.dims[0] && cq.dims[1] == ci.dims[1] && cq.dims[2] == ci.dims[2] &&
+          cq.precision == ci.precision) {
+        group.push_back(q);
+        done[q] = true;
+      }
+    }
+    const double cells = (double)ci.dims[0] * ci.dims[1] * ci.dims[2];
+    const double share = std::min(1.0, std::max(1e-3, cells / total_cells));
+    lcs_config pc = ci;  // the probe: flow only, unforced (zero fields), a fixed sweep count
+    pc.mode = LCS_MODE_FLOW;
+    pc.n_species = 0;
+    pc.forcing = LCS_FORCING_NO;
+    pc.itrmin = pc.itrmax = 20;
+    pc.use_graphs = 1;
+    std::vector<lcs_handle*> probes;
+    const int64_t n3 = (int64_t)ci.dims[0] * ci.dims[1] * ci.dims[2];
+    std::vector<double> zero((size_t)n3, 0.0);
+    for (size_t q = 0; q < group.size(); q++) {
+      lcs_handle* h = nullptr;
+      if (lcs_create(&pc, &h) != LCS_OK) break;
+      if (lcs_upload_flow(h, zero.data(), zero.data(), zero.data(), zero.data()) != LCS_OK) {
+        lcs_destroy(h);
+        break;
+      }
+      probes.push_back(h);
+    }
+    MemberTuning best;
+    best.share = share;
+    best.probe_ms = 1e300;
+    const int nz = ci.dims[2];
+    const int32_t rows_c[] = {13, 8, 5};
+    std::vector<int32_t> zc_c = {0};
+    for (int d : {1, 2, 4})
+      if (nz / d >= 8) zc_c.push_back((nz + 2) / d + 2);
+    // candidates: tile rows x (the cost model sized for the member's share or
+    // for the whole GPU, or a fixed chunk)
+    struct Cand { int32_t rows, zc; double share; };
+    std::vector<Cand> cands;
+    for (int32_t rows : rows_c) {
+      cands.push_back({rows, 0, share});
+      cands.push_back({rows, 0, 1.0});
+      for (int32_t zc : zc_c)
+        if (zc > 0) cands.push_back({rows, zc, share});
+    }
+    for (const Cand& cd : cands) {
+      bool ok = !probes.empty();
+      for (lcs_handle* h : probes) ok = ok && lcs_set_tuning(h, cd.rows, cd.zc, cd.share) == LCS_OK;
+      for (int rep = 0; ok && rep < 2; rep++) {  // rep 0 captures the graphs; rep 1 is timed
+        const auto t0 = Clock::now();
+        size_t begun = 0;
+        for (; begun < probes.size() && ok; begun++) ok = lcs_step_begin(probes[begun], 1) == LCS_OK;
+        for (size_t q = 0; q < begun; q++) ok = lcs_step_finish(probes[q], nullptr) == LCS_OK && ok;
+        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        if (ok && rep == 1 && ms < best.probe_ms) {
+          best.rw_rows = cd.rows;
+          best.zchunk = cd.zc;
+          best.share = cd.share;
+          best.probe_ms = ms;
+        }
+      }
+    }
+    for (lcs_handle* h : probes) lcs_destroy(h);
+    if (best.probe_ms >= 1e300) {  // no probe could run: the built-in shapes
+      best.rw_rows = 0;
+      best.zchunk = 0;
+      best.share = 1.0;
+      best.probe_ms = 0.0;
+    }
+    for (size_t q : group) {
+      const int rc = lcs_set_tuning(b->members[q], best.rw_rows, best.zchunk, best.share);
+      if (rc != LCS_OK) return serve_fail(rc, "batch member " + std::to_string(q) + ": " + handle_error(b->members[q]));
+      b->tuning[q] = best;
+    }
+  }
+  return LCS_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -70,8 +176,30 @@ int lcs_batch_create(const lcs_config* members, int32_t m, lcs_batch** out) {
       return serve_fail(rc, "batch member " + std::to_string(i) + ": " + why);
     }
     b->members.push_back(h);
+    b->cfgs.push_back(c);
   }
+  b->tuning.resize(b->members.size());
+  const char* tune = std::getenv("LCS_BATCH_TUNE");
+  if (!(tune && std::string(tune) == "0")) {
+    const int rc = autotune(b.get());
+    if (rc != LCS_OK) {
+      for (lcs_handle* q : b->members) lcs_destroy(q);
+      return rc;
+    }
+  }  // else: the built-in shapes of a solo run
   *out = b.release();
+  return LCS_OK;
+}
+
+int lcs_batch_tuning(const lcs_batch* b, int32_t i, int32_t* rw_rows, int32_t* zchunk, double* share,
+                     double* probe_ms) {
+  if (!b) return serve_fail(LCS_EINVAL, "null batch");
+  if (i < 0 || i >= (int32_t)b->members.size()) return serve_fail(LCS_EINVAL, "member index out of range");
+  const MemberTuning& t = b->tuning[i];
+  if (rw_rows) *rw_rows = t.rw_rows;
+  if (zchunk) *zchunk = t.zchunk;
+  if (share) *share = t.share;
+  if (probe_ms) *probe_ms = t.probe_ms;
   return LCS_OK;
 }
 

@@ -197,11 +197,13 @@ PROTOTYPES = {
     "lcs_step_poll": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "lcs_step_finish": (C.c_int, [_P, C.POINTER(Log)]),
     "lcs_device_bytes": (C.c_int, [_P, _I64]),
+    "lcs_set_tuning": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_double]),
     "lcs_batch_create": (C.c_int, [C.POINTER(Config), C.c_int32, C.POINTER(_P)]),
     "lcs_batch_size": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "lcs_batch_member": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
     "lcs_batch_step": (C.c_int, [_P, C.c_int32, C.POINTER(Log)]),
     "lcs_batch_destroy": (None, [_P]),
+    "lcs_batch_tuning": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _D, _D]),
     "lcs_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(_P)]),
     "lcs_server_submit": (C.c_int, [_P, C.POINTER(Request), _I64]),
     "lcs_server_poll": (C.c_int, [_P, C.c_int64, C.POINTER(C.c_int32), _I64]),

@@ -44,6 +44,14 @@ class Batch:
     def __len__(self):
         return len(self.members)
 
+    def tuning(self, i: int) -> dict:
+        """The launch shapes the batch's autotuner chose for member i."""
+        rows, zc = C.c_int32(), C.c_int32()
+        share, ms = C.c_double(), C.c_double()
+        _serve_check(self.lib, self.lib.lcs_batch_tuning(self.handle, i, C.byref(rows), C.byref(zc), C.byref(share),
+                                                         C.byref(ms)))
+        return {"rw_rows": rows.value, "zchunk": zc.value, "share": share.value, "probe_ms": ms.value}
+
     def step(self, nsteps: int) -> list:
         """nsteps of every member; returns logs[member][step] as dicts."""
         m = len(self.members)

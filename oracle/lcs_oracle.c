@@ -1097,6 +1097,13 @@ int lcs_step_finish(lcs_handle* h, lcs_log* logs) {
   if (logs) memcpy(logs, h->async_logs, (size_t)n * sizeof(lcs_log));
   return LCS_OK;
 }
+/* Launch shapes do not exist on the CPU: checked and ignored. */
+int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, double share) {
+  if (!h) return LCS_EINVAL;
+  if ((rw_rows != 0 && rw_rows != 13 && rw_rows != 8 && rw_rows != 5) || zchunk < 0 || !(share > 0.0 && share <= 1.0))
+    return fail(h, LCS_EINVAL, "bad tuning");
+  return LCS_OK;
+}
 int lcs_device_bytes(lcs_handle* h, int64_t* bytes) {
   if (!h || !bytes) return LCS_EINVAL;
   return lcs_footprint(&h->cfg, bytes);

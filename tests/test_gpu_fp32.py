@@ -10,7 +10,7 @@ not bit-comparable with FP64, so each test states its tolerance:
   kernels agree to 2e-6 (they contract multiply-adds differently); P, a sum of
   increments dp/dt that largely cancel, to 1e-3 (measured 2e-5);
 - ten full steps with forcing and particles: rel-L2 <= 1e-4 for U, V, W (the
-  north-star bound for the precision form; measured 4.4e-7) and <= 1e-3 for
+  bound stated for the precision form; measured 4.4e-7) and <= 1e-3 for
   P, particle positions <= 1e-6 and velocities <= 1e-4.
 """
 

@@ -3,7 +3,7 @@
 Element-wise stages compile without FMA contraction on both sides, so the
 FP64 fields must agree bit for bit; quantities that pass through a mean
 (forcing amplitudes, HSMAC residual) agree to 1e-12 relative, and after 10
-full steps the fields agree to the north-star bound rel-L2 <= 1e-10.
+full steps the fields agree to rel-L2 <= 1e-10, the plain method's parity bound.
 """
 
 import math

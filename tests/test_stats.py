@@ -1,0 +1,45 @@
+"""Host statistics (the restated `Flows.stat`, src/flows/stat.jl:66-153, and
+E(k)) on fields with analytic answers."""
+
+import math
+
+import numpy as np
+
+from lcs_b200 import stats
+
+
+def grid(n):
+    x = (np.arange(n) + 0.5) * 2 * math.pi / n
+    return np.meshgrid(x, x, x, indexing="ij")  # [k, j, i] order: z, y, x
+
+
+def test_shear_mode_urms_and_dissipation():
+    n, nu = 32, 0.01
+    z, y, x = grid(n)
+    U = np.sin(y)
+    V = np.zeros_like(U)
+    W = np.zeros_like(U)
+    st = stats.flow_stat(U, V, W, nu)
+    assert math.isclose(st["urms"], math.sqrt(0.5 / 3), rel_tol=1e-12)
+    assert math.isclose(st["k"], 0.25, rel_tol=1e-12)
+    # s12 = cos(y)/2 up to the o4 stencil error (~(dx^4) k^4 * 3/640): s2 = 4 <s12^2> = 1/2
+    assert math.isclose(st["epsilon"], 0.5 * nu, rel_tol=1e-4)
+
+
+def test_energy_spectrum_of_single_modes():
+    n = 32
+    z, y, x = grid(n)
+    U = np.cos(3 * x)          # energy <u^2>/2 = 1/4 at |k| = 3
+    V = 2.0 * np.sin(5 * z)    # energy 1 at |k| = 5
+    W = np.zeros_like(U)
+    e = stats.energy_spectrum(U, V, W)
+    assert math.isclose(e[3], 0.25, rel_tol=1e-12)
+    assert math.isclose(e[5], 1.0, rel_tol=1e-12)
+    assert math.isclose(e.sum(), 1.25, rel_tol=1e-12)
+    # Parseval: sum of E(k) = <|u|^2> / 2
+    assert math.isclose(e.sum(), 0.5 * float(np.mean(U ** 2 + V ** 2 + W ** 2)), rel_tol=1e-12)
+
+
+def test_particle_rms():
+    u = np.array([1.0, -1.0]); v = np.zeros(2); w = np.zeros(2)
+    assert math.isclose(stats.particle_rms_velocity(u, v, w), math.sqrt(1 / 3), rel_tol=1e-15)

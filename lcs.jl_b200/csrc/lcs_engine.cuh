@@ -602,6 +602,31 @@ class Engine : public EngineBase {
     }
     return zchunk_force > 0 ? std::min(zchunk_force, nzc) : (nzc + best_nc - 1) / best_nc;
   }
+  // Schedule of a row-warp sweep: chunks of zc planes per tile column, chunk
+  // major, in full waves of the resident CTAs; the chunks of a last, partial
+  // wave are split into q sub-ranges so that it fills the GPU too.  zc
+  // minimises the cost in plane-steps: full waves x (zc + 4 warm-up/drain
+  // planes) + the last wave's (sub-range + 4).
+  RwSched rw_schedule(int ncols, int nzc, int slots) const {
+    slots = share_slots(slots);
+    RwSched best{ncols, nzc, ncols, 1, ncols};
+    double best_cost = 1e300;
+    for (int nc = 1; nc <= std::min(nzc, 64); nc++) {
+      const int zc = zchunk_force > 0 ? std::min(zchunk_force, nzc) : (nzc + nc - 1) / nc;
+      const int nch = (nzc + zc - 1) / zc;
+      const int items = ncols * nch;
+      const int waves = items / slots, rem = items - waves * slots;
+      int q = rem > 0 ? std::max(1, slots / rem) : 1;
+      q = std::max(1, std::min(q, zc / 2));  // sub-ranges of 2 planes at least
+      const double cost = waves * (zc + 4.0) + (rem > 0 ? std::ceil((double)zc / q) + 4.0 : 0.0);
+      if (cost < best_cost - 1e-9) {
+        best_cost = cost;
+        best = RwSched{ncols, zc, waves * slots, q, waves * slots + rem * q};
+      }
+      if (zchunk_force > 0) break;
+    }
+    return best;
+  }
   // row-warp sweep: tiles of RW_TX x RTY whose first column is odd
   int fused_rw(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
     if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
@@ -613,18 +638,18 @@ class Engine : public EngineBase {
     while (((xo % am) + am) % am != ar % am) xo--;
     const int gx = (gb.hi[0] - xo + 1 + RW_TX - 1) / RW_TX, gy = (gb.len(1) + RTY - 1) / RTY;
     const int nzc = gb.len(2), ncols = gx * gy;
-    const int zc = pick_zchunk(nzc, ncols, num_sms * rw_ctas_per_sm);
-    const int nitems = ncols * ((nzc + zc - 1) / zc);
+    const RwSched sc = rw_schedule(ncols, nzc, num_sms * rw_ctas_per_sm);
+    const int nitems = sc.nitems;
     if (nitems > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
     if (nblocks) *nblocks = nitems;
     const dim3 grid(nitems), block(rw_threads);
     switch (rw_variant) {
       case 1: return launch("hsmac_rw", k_hsmac_rw<T, 8, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P, D,
-                            out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+                            out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
       case 2: return launch("hsmac_rw", k_hsmac_rw<T, 5, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P, D,
-                            out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+                            out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
       default: return launch("hsmac_rw", k_hsmac_rw<T, 13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P,
-                             D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
+                             D, out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
     }
   }
   int fused_tma(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {

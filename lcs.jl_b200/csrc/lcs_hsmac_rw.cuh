@@ -102,6 +102,32 @@ __device__ __forceinline__ T face_update_t(T val, bool lower_first, bool ma, T d
   return val;
 }
 
+// Work items of a sweep: (tile column, z range), chunk major.  The first
+// `full` items are whole chunks of `zc` planes; every later chunk is split into
+// q sub-ranges, so that the last wave of CTAs is as full as the first.
+struct RwSched {
+  int ncols, zc, full, q, nitems;
+};
+
+// The item's column and planes kb..ke (an empty range when kb > ke).
+__device__ __forceinline__ void rw_item(const RwSched& sc, int lo, int hi, int item, int* col, int* kb, int* ke) {
+  int i = item, sub = 0;
+  if (item >= sc.full) {
+    i = sc.full + (item - sc.full) / sc.q;
+    sub = (item - sc.full) % sc.q;
+  }
+  *col = i % sc.ncols;
+  const int kb0 = lo + (i / sc.ncols) * sc.zc, ke0 = min(hi, kb0 + sc.zc - 1);
+  if (item < sc.full) {
+    *kb = kb0;
+    *ke = ke0;
+    return;
+  }
+  const int len = (ke0 - kb0 + sc.q) / sc.q;  // ceil((ke0 - kb0 + 1) / q)
+  *kb = kb0 + sub * len;
+  *ke = min(ke0, *kb + len - 1);
+}
+
 // Per-lane (x) and per-warp (y) membership bits of one tile.
 struct RwBits {
   // x, this lane's pair (L = x0-2+2l, R = L+1)
@@ -124,7 +150,7 @@ struct RwBits {
 template <typename T, int TY, int NS>
 __global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::MINB)
     k_hsmac_rw(Ctx* __restrict__ ctx, Grid g, int set, const __grid_constant__ TensorMaps tm,
-               T* __restrict__ P, Box D, Box out, Box gb, int x_origin, int gx, int gy, int zc, int nitems,
+               T* __restrict__ P, Box D, Box out, Box gb, int x_origin, int gx, int gy, RwSched sc,
                HsmacCoef cf, double* __restrict__ partials, int finalize, int group_end) {
   using L = RwLayout<T, TY, NS>;
   using T2 = pair_t<T>;
@@ -157,13 +183,12 @@ __global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    const int ncols = gx * gy;
     int loads = 0;  // plane loads issued by this CTA: slot = index % NS, parity = (index / NS) & 1
     bool ok = true;
-    for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
-      const int col = item % ncols;
-      const int kb = gb.lo[2] + (item / ncols) * zc;
-      const int ke = min(gb.hi[2], kb + zc - 1);
+    for (int item = blockIdx.x; item < sc.nitems && ok; item += gridDim.x) {
+      int col, kb, ke;
+      rw_item(sc, gb.lo[2], gb.hi[2], item, &col, &kb, &ke);
+      if (kb > ke) continue;  // an empty sub-range (uniform in the CTA)
       const int x0 = x_origin + (col % gx) * RW_TX;
       const int y0 = gb.lo[1] + (col / gx) * TY;
       const int cx = x0 - 2 - 1 + A, cy = y0 - 2 + h - 1;

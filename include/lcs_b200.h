@@ -222,6 +222,19 @@ LCS_API int lcs_launch_count(lcs_handle* h, int64_t* launches);
 LCS_API int lcs_transfer_stats(lcs_handle* h, int64_t* h2d_bytes, int64_t* d2h_bytes);
 LCS_API int lcs_synchronize(lcs_handle* h);
 
+/* ---- statistics ----------------------------------------------------------
+ * `Flows.stat` (src/flows/stat.jl:66-153) on the device, on Us: the Summary
+ * (mean, max, min) of U, V, W, and k, epsilon, tau_eta, lambda (l_mu), l_eta,
+ * Re_lambda, u' (urms), k_eta, skewness and flatness of du/dx.  Reductions in
+ * FP64 in both precision forms; the halo is read through periodic wrapping, so
+ * the call changes no state.  The integral length L and C_epsilon are 0, as in
+ * the reference without an integral-length buffer (stat.jl:155). */
+typedef struct lcs_flow_stats {
+  double u_mean, u_max, u_min, v_mean, v_max, v_min, w_mean, w_max, w_min;
+  double k, epsilon, tau_eta, l_mu, l_eta, Re_lambda, urms, k_eta, skewness, flatness, L, C_epsilon;
+} lcs_flow_stats;
+LCS_API int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* out);
+
 /* ---- asynchronous steps (no reference counterpart) ----------------------
  * For hosts that drive many handles at once (the batching and serving forms
  * below, or a Julia task per handle).  lcs_step_begin enqueues nsteps

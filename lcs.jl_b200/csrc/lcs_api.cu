@@ -159,6 +159,7 @@ int lcs_step_poll(lcs_handle* h, int32_t* done) {
   return rc;
 }
 int lcs_step_finish(lcs_handle* h, lcs_log* logs) { H(h); return h->e->step_finish(logs); }
+int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* out) { H(h); return h->e->flow_stat(out); }
 int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, double share) {
   H(h);
   return h->e->set_tuning(rw_rows, zchunk, share);

@@ -36,6 +36,7 @@ struct EngineBase {
   virtual int step_finish(lcs_log* logs) = 0;
   virtual int64_t device_bytes() const = 0;
   virtual int set_tuning(int rw_rows, int zchunk, double share) = 0;
+  virtual int flow_stat(lcs_flow_stats* out) = 0;
   virtual int transfer_stats(int64_t* h2d, int64_t* d2h) = 0;
   virtual int synchalo(int mask, int r, int full) = 0;
   virtual int rhs(int stage) = 0;

@@ -1362,6 +1362,42 @@ class Engine : public EngineBase {
     if (dt) *dt = hctx->scal[7];
     return LCS_OK;
   }
+  int flow_stat(lcs_flow_stats* out) override {
+    LCS_TRY(check_flow());
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    if (!out) return fail(LCS_EINVAL, "null output");
+    const int64_t total = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const unsigned int nb = blocks_for(total, 256, 148 * 8);
+    LCS_TRY(launch("flow_stat", k_flow_stat<T>, dim3(nb), dim3(256), 0, (const Ctx*)dctx, g, hc.dxi, hc.dyi, hc.dzi,
+                   partials));
+    LCS_TRY(launch("flow_stat_final", k_flow_stat_final, dim3(1), dim3(256), 0, (const double*)partials, (int)nb,
+                   stage));
+    double v[kStatVals];
+    LCS_TRY(copy(v, stage, sizeof v, cudaMemcpyDeviceToHost));
+    LCS_TRY(collect_profile());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    const double N = (double)total;
+    lcs_flow_stats& o = *out;
+    o.u_mean = v[5] / N; o.v_mean = v[6] / N; o.w_mean = v[7] / N;
+    o.u_max = v[8]; o.v_max = v[9]; o.w_max = v[10];
+    o.u_min = v[11]; o.v_min = v[12]; o.w_min = v[13];
+    const double u2 = v[0] / N, s2 = v[1] / N, d2 = v[2] / N, d3 = v[3] / N, d4 = v[4] / N;
+    const double Re = cfg.U0 * cfg.L0 / cfg.NU;  // Flows.Re(params)
+    // stat.jl:135-151
+    o.urms = std::sqrt(u2 / 3.0);
+    o.k = 0.5 * (u2 - o.u_mean * o.u_mean - o.v_mean * o.v_mean - o.w_mean * o.w_mean);
+    o.epsilon = s2 / Re;
+    o.tau_eta = std::sqrt(1.0 / o.epsilon / Re);
+    o.l_mu = std::sqrt(15.0 * o.urms * o.urms / o.epsilon / Re);
+    o.l_eta = std::pow(1.0 / o.epsilon / (Re * Re * Re), 0.25);
+    o.Re_lambda = o.l_mu * o.urms * Re;
+    o.k_eta = (std::min(g.n[0], std::min(g.n[1], g.n[2])) / 2.0) * o.l_eta;
+    o.skewness = -d3 / std::pow(d2, 1.5);
+    o.flatness = d4 / (d2 * d2);
+    o.L = 0.0;
+    o.C_epsilon = 0.0;
+    return LCS_OK;
+  }
   int particles_timestep(double* dt) override {
     LCS_TRY(read_ctx());
     if (dt) *dt = (cfg.mode == LCS_MODE_FLOW_PARTICLE && cfg.n_species > 0) ? hctx->dt_particles : cfg.dtmax;

@@ -815,6 +815,99 @@ __global__ void __launch_bounds__(256) k_cfl_max(const Ctx* __restrict__ ctx, Gr
   }
 }
 
+// --------------------------------------------------------------------------
+// flow statistics (src/flows/stat.jl:66-138): per interior cell the squared
+// speed u2, the strain-rate invariant s2 = 2 S_ij S_ij and du/dx^2,3,4 with
+// the fourth-order half-point derivatives of src/diff.jl, read with periodic
+// wrapping (the reference fills a FullHalo first); block sums in FP64 plus
+// the mean, max and min of U, V, W.  14 values per block:
+// sum u2, s2, d2, d3, d4, sum U, V, W, max U, V, W, min U, V, W.
+// --------------------------------------------------------------------------
+constexpr int kStatVals = 14;
+
+template <typename T>
+__device__ __forceinline__ double d1o4(const T* A, int64_t c0, int64_t c1, int64_t c2, int64_t c3) {
+  return (1.0 / 24.0) * ((double)A[c0] - 27.0 * (double)A[c1] + 27.0 * (double)A[c2] - (double)A[c3]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_flow_stat(const Ctx* __restrict__ ctx, Grid g, double dxi, double dyi,
+                                                   double dzi, double* __restrict__ partials) {
+  __shared__ double sh[8];
+  const T* U = (const T*)ctx->vel[kSetUs][0];
+  const T* V = (const T*)ctx->vel[kSetUs][1];
+  const T* W = (const T*)ctx->vel[kSetUs][2];
+  const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+  const int64_t total = (int64_t)nx * ny * nz;
+  double acc[kStatVals];
+  for (int q = 0; q < 8; q++) acc[q] = 0.0;
+  for (int q = 8; q < 11; q++) acc[q] = -INFINITY;
+  for (int q = 11; q < 14; q++) acc[q] = INFINITY;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % nx);
+    const int j = 1 + (int)((t / nx) % ny);
+    const int k = 1 + (int)(t / ((int64_t)nx * ny));
+    auto at = [&](int a, int b, int c) { return g.at(wrap1(a, nx), wrap1(b, ny), wrap1(c, nz)); };
+    const int64_t c = g.at(i, j, k);
+    const double u = (double)U[c], v = (double)V[c], w = (double)W[c];
+    const double u2 = u * u + v * v + w * w;
+    // stat.jl:90-103
+    const double dudx = dxi * d1o4(U, at(i - 2, j, k), at(i - 1, j, k), c, at(i + 1, j, k));
+    const double dvdy = dyi * d1o4(V, at(i, j - 2, k), at(i, j - 1, k), c, at(i, j + 1, k));
+    const double dwdz = dzi * d1o4(W, at(i, j, k - 2), at(i, j, k - 1), c, at(i, j, k + 1));
+    const double dudy = dyi * d1o4(U, at(i, j - 2, k), at(i, j - 1, k), c, at(i, j + 1, k));
+    const double dvdx = dxi * d1o4(V, at(i - 1, j - 1, k), at(i, j - 1, k), at(i + 1, j - 1, k), at(i + 2, j - 1, k));
+    const double dvdz = dzi * d1o4(V, at(i, j - 1, k - 1), at(i, j - 1, k), at(i, j - 1, k + 1), at(i, j - 1, k + 2));
+    const double dwdy = dyi * d1o4(W, at(i, j - 2, k), at(i, j - 1, k), c, at(i, j + 1, k));
+    const double dwdx = dxi * d1o4(W, at(i - 1, j, k - 1), at(i, j, k - 1), at(i + 1, j, k - 1), at(i + 2, j, k - 1));
+    const double dudz = dzi * d1o4(U, at(i, j, k - 2), at(i, j, k - 1), c, at(i, j, k + 1));
+    const double s11 = 0.5 * (dudx + dudx), s22 = 0.5 * (dvdy + dvdy), s33 = 0.5 * (dwdz + dwdz);
+    const double s12 = 0.5 * (dudy + dvdx), s13 = 0.5 * (dudz + dwdx), s23 = 0.5 * (dvdz + dwdy);
+    const double s2 = 2.0 * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23));
+    const double d2 = dudx * dudx;
+    acc[0] += u2;
+    acc[1] += s2;
+    acc[2] += d2;
+    acc[3] += d2 * dudx;
+    acc[4] += d2 * d2;
+    acc[5] += u;
+    acc[6] += v;
+    acc[7] += w;
+    acc[8] = fmax(acc[8], u);
+    acc[9] = fmax(acc[9], v);
+    acc[10] = fmax(acc[10], w);
+    acc[11] = fmin(acc[11], u);
+    acc[12] = fmin(acc[12], v);
+    acc[13] = fmin(acc[13], w);
+  }
+  for (int q = 0; q < kStatVals; q++) {
+    double r;
+    if (q < 8) {
+      r = block_sum<256>(acc[q], sh);
+    } else if (q < 11) {
+      r = block_max<256>(acc[q], sh);
+    } else {
+      r = -block_max<256>(-acc[q], sh);
+    }
+    if (threadIdx.x == 0) partials[kStatVals * blockIdx.x + q] = r;
+  }
+}
+
+// Combine the block values in a fixed order (1 block); result in out[0..13].
+__global__ void __launch_bounds__(256) k_flow_stat_final(const double* __restrict__ partials, int nb,
+                                                         double* __restrict__ out) {
+  __shared__ double sh[8];
+  for (int q = 0; q < kStatVals; q++) {
+    double v = q < 8 ? 0.0 : (q < 11 ? -INFINITY : INFINITY);
+    for (int b = threadIdx.x; b < nb; b += 256) {
+      const double x = partials[kStatVals * b + q];
+      v = q < 8 ? v + x : (q < 11 ? fmax(v, x) : fmin(v, x));
+    }
+    const double r = q < 8 ? block_sum<256>(v, sh) : (q < 11 ? block_max<256>(v, sh) : -block_max<256>(-v, sh));
+    if (threadIdx.x == 0) out[q] = r;
+  }
+}
+
 struct DtCoef {
   double cfl, dtmax, dx, dy, dz, Re;
   int with_particles;

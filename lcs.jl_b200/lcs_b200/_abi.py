@@ -119,6 +119,15 @@ _D = C.POINTER(C.c_double)
 _I64 = C.POINTER(C.c_int64)
 
 
+class FlowStat(C.Structure):
+    _fields_ = [(f, C.c_double) for f in (
+        "u_mean", "u_max", "u_min", "v_mean", "v_max", "v_min", "w_mean", "w_max", "w_min", "k", "epsilon",
+        "tau_eta", "l_mu", "l_eta", "Re_lambda", "urms", "k_eta", "skewness", "flatness", "L", "C_epsilon")]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 # ---- batching and serving forms (include/lcs_b200.h) -----------------------
 MAX_ASYNC_STEPS = 4096
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
@@ -193,6 +202,7 @@ PROTOTYPES = {
     "lcs_synchronize": (C.c_int, [_P]),
     "lcs_flow_timestep_noalloc": (C.c_int, [_P, _P, _P, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_double,
                                             C.c_double, _P, _P]),
+    "lcs_flow_stat": (C.c_int, [_P, C.POINTER(FlowStat)]),
     "lcs_step_begin": (C.c_int, [_P, C.c_int32]),
     "lcs_step_poll": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "lcs_step_finish": (C.c_int, [_P, C.POINTER(Log)]),

@@ -174,6 +174,12 @@ class Engine:
         self._check(self.lib.lcs_step(self.handle, nsteps, arr if logs else None))
         return [arr[q].as_dict() for q in range(nsteps)] if logs else None
 
+    def flow_stat(self) -> dict:
+        """`Flows.stat` (src/flows/stat.jl:66-153) computed on the device."""
+        st = _abi.FlowStat()
+        self._check(self.lib.lcs_flow_stat(self.handle, C.byref(st)))
+        return st.as_dict()
+
     def step_timed(self, nsteps: int, logs: bool = True):
         """`step`, returning (logs, device milliseconds of the nsteps)."""
         arr = (_abi.Log * max(1, nsteps))() if logs else None

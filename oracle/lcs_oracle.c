@@ -1097,6 +1097,65 @@ int lcs_step_finish(lcs_handle* h, lcs_log* logs) {
   if (logs) memcpy(logs, h->async_logs, (size_t)n * sizeof(lcs_log));
   return LCS_OK;
 }
+/* `Flows.stat` (src/flows/stat.jl:66-153): per-cell squared speed, strain
+ * invariant and du/dx moments with the o4 half-point derivative (src/diff.jl),
+ * halo reads by periodic wrapping; sums in the order i, j, k. */
+static double d1o4(double a, double b, double c, double d) { return (1.0 / 24.0) * (a - 27.0 * b + 27.0 * c - d); }
+static int wrapi(int i, int n) { int r = (i - 1) % n; return (r < 0 ? r + n : r) + 1; }
+int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* o) {
+  if (!h || !o) return LCS_EINVAL;
+  const grid_t* g = &h->g;
+  const int nx = g->n[0], ny = g->n[1], nz = g->n[2];
+  const double dxi = 1.0 / spacing(g, 0), dyi = 1.0 / spacing(g, 1), dzi = 1.0 / spacing(g, 2);
+  const double *U = h->U, *V = h->V, *W = h->W;
+#define A(F, a, b, c) F[IX(g, wrapi(a, nx), wrapi(b, ny), wrapi(c, nz))]
+  double su2 = 0, ss2 = 0, sd2 = 0, sd3 = 0, sd4 = 0, su = 0, sv = 0, sw = 0;
+  double mxu = -INFINITY, mxv = -INFINITY, mxw = -INFINITY, mnu = INFINITY, mnv = INFINITY, mnw = INFINITY;
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        const double u = A(U, i, j, k), v = A(V, i, j, k), w = A(W, i, j, k);
+        const double dudx = dxi * d1o4(A(U, i - 2, j, k), A(U, i - 1, j, k), u, A(U, i + 1, j, k));
+        const double dvdy = dyi * d1o4(A(V, i, j - 2, k), A(V, i, j - 1, k), v, A(V, i, j + 1, k));
+        const double dwdz = dzi * d1o4(A(W, i, j, k - 2), A(W, i, j, k - 1), w, A(W, i, j, k + 1));
+        const double dudy = dyi * d1o4(A(U, i, j - 2, k), A(U, i, j - 1, k), u, A(U, i, j + 1, k));
+        const double dvdx = dxi * d1o4(A(V, i - 1, j - 1, k), A(V, i, j - 1, k), A(V, i + 1, j - 1, k), A(V, i + 2, j - 1, k));
+        const double dvdz = dzi * d1o4(A(V, i, j - 1, k - 1), A(V, i, j - 1, k), A(V, i, j - 1, k + 1), A(V, i, j - 1, k + 2));
+        const double dwdy = dyi * d1o4(A(W, i, j - 2, k), A(W, i, j - 1, k), w, A(W, i, j + 1, k));
+        const double dwdx = dxi * d1o4(A(W, i - 1, j, k - 1), A(W, i, j, k - 1), A(W, i + 1, j, k - 1), A(W, i + 2, j, k - 1));
+        const double dudz = dzi * d1o4(A(U, i, j, k - 2), A(U, i, j, k - 1), u, A(U, i, j, k + 1));
+        const double s11 = 0.5 * (dudx + dudx), s22 = 0.5 * (dvdy + dvdy), s33 = 0.5 * (dwdz + dwdz);
+        const double s12 = 0.5 * (dudy + dvdx), s13 = 0.5 * (dudz + dwdx), s23 = 0.5 * (dvdz + dwdy);
+        ss2 += 2.0 * (s11 * s11 + s22 * s22 + s33 * s33 + 2.0 * (s12 * s12 + s13 * s13 + s23 * s23));
+        su2 += u * u + v * v + w * w;
+        const double d2 = dudx * dudx;
+        sd2 += d2; sd3 += d2 * dudx; sd4 += d2 * d2;
+        su += u; sv += v; sw += w;
+        mxu = fmax(mxu, u); mxv = fmax(mxv, v); mxw = fmax(mxw, w);
+        mnu = fmin(mnu, u); mnv = fmin(mnv, v); mnw = fmin(mnw, w);
+      }
+#undef A
+  const double N = (double)nx * ny * nz;
+  o->u_mean = su / N; o->v_mean = sv / N; o->w_mean = sw / N;
+  o->u_max = mxu; o->v_max = mxv; o->w_max = mxw; o->u_min = mnu; o->v_min = mnv; o->w_min = mnw;
+  const double u2 = su2 / N, s2 = ss2 / N, d2 = sd2 / N, d3 = sd3 / N, d4 = sd4 / N;
+  const double Re = h->cfg.U0 * h->cfg.L0 / h->cfg.NU;
+  o->urms = sqrt(u2 / 3.0);
+  o->k = 0.5 * (u2 - o->u_mean * o->u_mean - o->v_mean * o->v_mean - o->w_mean * o->w_mean);
+  o->epsilon = s2 / Re;
+  o->tau_eta = sqrt(1.0 / o->epsilon / Re);
+  o->l_mu = sqrt(15.0 * o->urms * o->urms / o->epsilon / Re);
+  o->l_eta = pow(1.0 / o->epsilon / (Re * Re * Re), 0.25);
+  o->Re_lambda = o->l_mu * o->urms * Re;
+  const int nmin = nx < ny ? (nx < nz ? nx : nz) : (ny < nz ? ny : nz);
+  o->k_eta = (nmin / 2.0) * o->l_eta;
+  o->skewness = -d3 / pow(d2, 1.5);
+  o->flatness = d4 / (d2 * d2);
+  o->L = 0.0;
+  o->C_epsilon = 0.0;
+  return LCS_OK;
+}
+
 /* Launch shapes do not exist on the CPU: checked and ignored. */
 int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, double share) {
   if (!h) return LCS_EINVAL;

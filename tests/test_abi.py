@@ -72,7 +72,7 @@ def test_struct_layout_matches_c():
 
 @pytest.mark.parametrize("cname,pyname", [("lcs_server_config", "ServerConfig"), ("lcs_species_state", "SpeciesState"),
                                           ("lcs_request", "Request"), ("lcs_species_out", "SpeciesOut"),
-                                          ("lcs_server_stats", "ServerStats")])
+                                          ("lcs_server_stats", "ServerStats"), ("lcs_flow_stats", "FlowStat")])
 def test_serving_struct_layouts_match_c(cname, pyname):
     st = getattr(_abi, pyname)
     fields = [f for f, _ in st._fields_]

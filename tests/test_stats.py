@@ -43,3 +43,28 @@ def test_energy_spectrum_of_single_modes():
 def test_particle_rms():
     u = np.array([1.0, -1.0]); v = np.zeros(2); w = np.zeros(2)
     assert math.isclose(stats.particle_rms_velocity(u, v, w), math.sqrt(1 / 3), rel_tol=1e-15)
+
+
+KEYS = ("urms", "k", "epsilon", "tau_eta", "l_mu", "l_eta", "Re_lambda", "k_eta", "skewness", "flatness")
+
+
+def test_oracle_flow_stat_equals_host_restatement():
+    """The oracle's lcs_flow_stat (C, sums in i, j, k order) against the numpy
+    restatement (pairwise sums): the same means to rounding."""
+    from helpers import make_config
+    from lcs_b200 import _abi, inits
+    from oracle_engine import OracleEngine
+
+    n, nu = 24, 0.01
+    e = OracleEngine(make_config(n, mode=_abi.MODE_FLOW, Re=1.0 / nu))
+    U, V, W, P = inits.spectral_flow(n, seed=3)
+    e.upload_flow(U, V, W, P)
+    got = e.flow_stat()
+    ref = stats.flow_stat(U, V, W, nu)
+    for k in KEYS:
+        assert math.isclose(got[k], ref[k], rel_tol=1e-12), (k, got[k], ref[k])
+    for c, a in zip("uvw", (U, V, W)):
+        assert math.isclose(got[c + "_mean"], float(a.mean()), rel_tol=1e-9, abs_tol=1e-15)
+        assert got[c + "_max"] == float(a.max()) and got[c + "_min"] == float(a.min())
+    assert got["L"] == 0.0 and got["C_epsilon"] == 0.0
+    e.close()

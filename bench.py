@@ -58,6 +58,8 @@ WORKLOADS = {
     # the 64-member ensemble and the served request stream: run_batch and run_serve
     "batch64": None,
     "serve": None,
+    # the particle cell index (makeindex!) of the lp512 particles, grid_ratio 4: run_makeindex
+    "makeindex": None,
 }
 
 # DRAM bytes (read + write) per launch of the sweep kernel, per interior cell:
@@ -594,6 +596,111 @@ def run_serve(args):
     return 0
 
 
+# ------------------------------------------------------------ particle cell index
+def makeindex_bytes(n, H):
+    """Algorithmic DRAM bytes of one makeindex of n particles over H cells, as
+    this design moves them: positions 24 + keys/indices 8 (cell_hash); the
+    stable LSD sort of 32-bit (hash, index) pairs, one histogram read 4 and 3
+    passes of 16 for hashes below 2^24 (radix_sort); perm 4 + 17 8-byte
+    properties read and written into the spare block (permute) 2 x 17 x 8;
+    keys 4 + Int64 hashes 8 (hash_runs); per cell the run-end array zeroed 8,
+    scanned 16 and read 8, starts/stops 16."""
+    return n * (24 + 8 + 4 + 3 * 16 + 4 + 2 * 17 * 8 + 4 + 8) + (H + 1) * (8 + 16 + 8) + H * 16
+
+
+def run_makeindex(args):
+    """`Particles.makeindex!` of the lp512 particles (512^3 grid, 2^24 particles
+    in 3 species, grid_ratio 4 as in the reference's cfgs/N1024-1.lcs-yaml):
+    particles indexed per second, on the order a previous index left after one
+    time step (the steady case; `value`, device-timed) and on random order (the
+    first index).  e2e is the host wall clock around the synchronous calls."""
+    from lcs_b200 import Engine
+
+    ratio = 4
+    rc, w = make_run_config("lp512", seed=0, precision="fp64")
+    rc.abi.use_graphs = 1
+    flow, parts = host_inputs(rc)
+    eng = Engine(rc.abi)
+    load_engine(eng, rc, flow, parts)
+    nsp = len(rc.species)
+    total = float(sum(si.nvalid for si in rc.species))
+    H = (512 // ratio + 2) ** 3
+    algo = float(sum(makeindex_bytes(si.nvalid, H) for si in rc.species))
+
+    def index_all():
+        for s in range(nsp):
+            eng.particles_makeindex(s, 1, ratio)
+
+    def device_ms():
+        t = eng.profile_totals()
+        return t["makeindex"][0], {k: v[0] for k, v in t.items()}
+
+    index_all()  # buffers allocated; the random order is restored below
+    eng.synchronize()
+    reps = max(1, min(args.steps, 3))
+    eng.profile(True)
+    eng.profile_reset()
+    for _ in range(reps):
+        for s, (d, x, y, z) in enumerate(parts):
+            zero = np.zeros_like(x)
+            eng.upload_particles(s, d, x, y, z, zero, zero, zero)
+        index_all()
+    first_ms = device_ms()[0] / reps
+    eng.profile(False)
+    for _ in range(args.warmup):
+        index_all()
+    eng.step(1)
+    index_all()
+    eng.step(1)  # particles moved one step since their last index
+    eng.synchronize()
+    eng.profile(True)
+    eng.profile_reset()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        index_all()
+    wall_s = (time.perf_counter() - t0) / args.steps
+    steady_ms, parts_ms = device_ms()
+    steady_ms /= args.steps
+    eng.profile(False)
+    hashes, starts, stops = eng.particles_cellindex(0, ratio)
+    ok = bool(np.all(np.diff(hashes) >= 0)) and int(np.sum(stops - starts + 1)) == hashes.size
+    launches = eng.launch_count()
+    eng.close()
+    peak, peak_src = hbm_peak()
+    gbs = algo / (steady_ms * 1e-3) / 1e9
+    out = {
+        "metric": "particles indexed/s", "value": total / (steady_ms * 1e-3), "unit": "particles/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": steady_ms, "higher_is_better": True,
+        "dtype": "f64 positions, u32 keys", "data": "synthetic (seeded uniform positions)",
+        "config": {"workload": "makeindex", "n": 512, "particles": int(total), "species": nsp, "grid_ratio": ratio,
+                   "cells": int(H), "l2": "inputs (2^24 x 17 x 8 B) exceed L2"},
+        "e2e": {"value": total / wall_s, "unit": "particles/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0, "note": "host wall clock around the synchronous C-ABI calls"},
+        "first_index": {"value": total / (first_ms * 1e-3), "ms": first_ms, "note": "random particle order"},
+        "per_kernel_ms": {k: v / args.steps for k, v in parts_ms.items() if k != "makeindex"},
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                     "peak_source": peak_src, "algorithmic_bytes": algo},
+        "invariants_ok": ok, "gpu_launches_total": launches,
+        "timing": "CUDA events on the engine stream around each index (profiling spans)",
+    }
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_engine import OracleEngine
+
+        o = OracleEngine(rc.abi)
+        d, x, y, z = parts[0]
+        zero = np.zeros_like(x)
+        o.upload_particles(0, d, x, y, z, zero, zero, zero)
+        t0 = time.perf_counter()
+        o.particles_makeindex(0, 1, ratio)
+        el = time.perf_counter() - t0
+        o.close()
+        out["cpu_baseline"] = {"value": x.size / el, "unit": "particles/s", "cores": 1, "kind": "port",
+                               "sample": f"one makeindex of species 0 ({x.size} particles, random order, {el:.1f} s)"}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -618,6 +725,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "makeindex":
+        return run_makeindex(args)
     return run_b200(args)
 
 

@@ -235,6 +235,18 @@ typedef struct lcs_flow_stats {
 } lcs_flow_stats;
 LCS_API int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* out);
 
+/* `Particles.makeindex!` (src/particles/makeindex.jl:29-67) on species s with
+ * the positions of stage (1: xss, 2: xss2): cell index ci = floor(x / dxc) + 1
+ * per axis (dxc = (2pi/n) * grid_ratio, particles/config.jl:60), hash = the
+ * 1-based column-major index of ci over the cell axes 0:nc+1 (nc = n /
+ * grid_ratio), a stable sort of the species' particles by hash that permutes
+ * every property (the device order of the species changes; ids follow), and
+ * starts/stops of every hash 1..(nc+2)^3 (src/utils/fast.jl:8-40). */
+LCS_API int lcs_particles_makeindex(lcs_handle* h, int32_t species, int32_t stage, int32_t grid_ratio);
+/* The last cell index of species s: hashes[nvalid], starts[(nc+2)^3],
+ * stops[(nc+2)^3] (Int64, as LCS.IP); NULL pointers are skipped. */
+LCS_API int lcs_particles_cellindex(lcs_handle* h, int32_t species, int64_t* hashes, int64_t* starts, int64_t* stops);
+
 /* ---- asynchronous steps (no reference counterpart) ----------------------
  * For hosts that drive many handles at once (the batching and serving forms
  * below, or a Julia task per handle).  lcs_step_begin enqueues nsteps

@@ -160,6 +160,14 @@ int lcs_step_poll(lcs_handle* h, int32_t* done) {
 }
 int lcs_step_finish(lcs_handle* h, lcs_log* logs) { H(h); return h->e->step_finish(logs); }
 int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* out) { H(h); return h->e->flow_stat(out); }
+int lcs_particles_makeindex(lcs_handle* h, int32_t s, int32_t stage, int32_t ratio) {
+  H(h);
+  return h->e->particles_makeindex(s, stage, ratio);
+}
+int lcs_particles_cellindex(lcs_handle* h, int32_t s, int64_t* hashes, int64_t* starts, int64_t* stops) {
+  H(h);
+  return h->e->particles_cellindex(s, hashes, starts, stops);
+}
 int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, double share) {
   H(h);
   return h->e->set_tuning(rw_rows, zchunk, share);

@@ -37,6 +37,8 @@ struct EngineBase {
   virtual int64_t device_bytes() const = 0;
   virtual int set_tuning(int rw_rows, int zchunk, double share) = 0;
   virtual int flow_stat(lcs_flow_stats* out) = 0;
+  virtual int particles_makeindex(int s, int stage, int grid_ratio) = 0;
+  virtual int particles_cellindex(int s, int64_t* hashes, int64_t* starts, int64_t* stops) = 0;
   virtual int transfer_stats(int64_t* h2d, int64_t* d2h) = 0;
   virtual int synchalo(int mask, int r, int full) = 0;
   virtual int rhs(int stage) = 0;

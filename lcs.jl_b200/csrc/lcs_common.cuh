@@ -97,6 +97,7 @@ struct Ctx {
   int nonfinite;        // sticky: a NaN/Inf dt or residual was seen
   int wait_error;       // sticky: a bounded device wait (TMA copy, grid barrier) ran out
   unsigned int gbar_count, gbar_gen;  // grid-wide barrier of cooperative kernels
+  double* sp_base[16];  // property block of each species: 16 FP64 properties, then the ids
 };
 
 // ---- stencil primitives (src/diff.jl:1-39), same evaluation order --------

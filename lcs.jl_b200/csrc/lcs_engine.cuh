@@ -25,6 +25,7 @@
 #include "lcs_kernels.cuh"
 #include "lcs_hsmac_tma.cuh"
 #include "lcs_hsmac_rw.cuh"
+#include "lcs_makeindex.cuh"
 
 namespace lcs {
 
@@ -152,6 +153,23 @@ class Engine : public EngineBase {
   double2 *ph[3] = {nullptr, nullptr, nullptr};
   RcfModes modes;
   SpeciesDev sp[LCS_MAX_SPECIES];
+  // cell index of a species (makeindex!), allocated on its first use
+  struct CellIndex {
+    CellGeom cg{};
+    int ratio = 0;
+    int64_t H = 0;
+    int64_t* hashes = nullptr;
+    int64_t* starts = nullptr;  // and stops = starts + H
+    int64_t* S = nullptr;       // run ends S[0..H] and their max-scan M = S + H + 1
+    uint32_t* kv = nullptr;     // keys in/out, values in/out: 4 x n
+    void* temp = nullptr;       // CUB scratch of the sort and the scan
+    size_t temp_bytes = 0;
+    bool built = false;
+  } ci[LCS_MAX_SPECIES];
+  // A second property block per species (17 x n x 8 bytes, allocated on the
+  // first index): the permutation writes the spare block and the two swap.
+  uint64_t* sp_alloc[LCS_MAX_SPECIES] = {};  // owned (cudaMalloc)
+  uint64_t* sp_spare[LCS_MAX_SPECIES] = {};  // the block not in use (sp_alloc or the one in the pool)
   bool uploaded_flow = false;
   int64_t launches = 0;
   // profiling
@@ -187,6 +205,8 @@ class Engine : public EngineBase {
     for (auto e : event_pool) cudaEventDestroy(e);
     if (hctx) cudaFreeHost(hctx);
     if (hlogs) cudaFreeHost(hlogs);
+    for (auto& c : ci) free_index(c);
+    for (auto* a : sp_alloc) cudaFree(a);
     if (async_ev) cudaEventDestroy(async_ev);
     if (pool) cudaFree(pool);
     if (stream) cudaStreamDestroy(stream);
@@ -234,6 +254,8 @@ class Engine : public EngineBase {
         h0.vphys[s][q] = 3 * s + q;
       }
     h0.dt_particles = c.dtmax;
+    static_assert(sizeof(h0.sp_base) / sizeof(h0.sp_base[0]) == LCS_MAX_SPECIES, "one block per species");
+    for (int s = 0; s < c.n_species; s++) h0.sp_base[s] = (double*)(pool + plan.off_sp[s]);
     h0.cur.p = NAN;
     h0.cur.e10 = NAN;
     *hctx = h0;
@@ -857,7 +879,7 @@ class Engine : public EngineBase {
       if (only >= 0 && s != only) continue;
       if (sp[s].n == 0) continue;
       LCS_TRY(launch("particles", k_particles<T>, dim3((unsigned)((sp[s].n + 255) / 256)), dim3(256), 0,
-                     (const Ctx*)dctx, g, sp[s], pc, stage, modes_mask, use_stage_dt, dt));
+                     (const Ctx*)dctx, g, s, sp[s], pc, stage, modes_mask, use_stage_dt, dt));
     }
     return LCS_OK;
   }
@@ -1398,6 +1420,127 @@ class Engine : public EngineBase {
     o.C_epsilon = 0.0;
     return LCS_OK;
   }
+  static void free_index(CellIndex& c) {
+    cudaFree(c.hashes);
+    cudaFree(c.starts);
+    cudaFree(c.S);
+    cudaFree(c.kv);
+    cudaFree(c.temp);
+    c = CellIndex{};
+  }
+  // a device-timed span of library calls under a label (when profiling)
+  template <typename F>
+  int timed(const char* label, F&& f) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (prof && !capturing) {
+      a = get_event();
+      b = get_event();
+      cudaEventRecord(a, stream);
+    }
+    cudaError_t e = f();
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(LCS_ECUDA, "%s: %s", label, cudaGetErrorString(e));
+    if (a) {
+      cudaEventRecord(b, stream);
+      recs.push_back({label, a, b});
+    }
+    return LCS_OK;
+  }
+  // `Particles.makeindex!` (src/particles/makeindex.jl:29-67) on species s
+  // with the positions of `stage`; the species' device order becomes the
+  // sorted one.
+  int particles_makeindex(int s, int stage_, int ratio) override {
+    LCS_TRY(check_species(s));
+    LCS_TRY(check_stage(stage_));
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    if (ratio < 1 || g.n[0] % ratio || g.n[1] % ratio || g.n[2] % ratio)
+      return fail(LCS_EINVAL, "grid_ratio must be positive and divide the grid dims");
+    CellIndex& c = ci[s];
+    const int64_t n = sp[s].n;
+    CellGeom cg;
+    int64_t H = 1;
+    for (int a = 0; a < 3; a++) {
+      cg.nc[a] = g.n[a] / ratio;
+      cg.dxc[a] = (kDomainLength / g.n[a]) * ratio;  // LCS.spacings(grid) .* grid_ratio
+      H *= cg.nc[a] + 2;
+    }
+    if (H > (int64_t)UINT32_MAX || n > (int64_t)UINT32_MAX) return fail(LCS_EINVAL, "cell index too large");
+    if (c.ratio != ratio) {  // (re)allocate for this cell size
+      LCS_CUDA(cudaStreamSynchronize(stream));
+      free_index(c);
+      const size_t nn = (size_t)std::max<int64_t>(n, 1);
+      LCS_CUDA(cudaMalloc(&c.hashes, nn * sizeof(int64_t)));
+      LCS_CUDA(cudaMalloc(&c.starts, (size_t)2 * H * sizeof(int64_t)));
+      LCS_CUDA(cudaMalloc(&c.S, (size_t)2 * (H + 1) * sizeof(int64_t)));
+      LCS_CUDA(cudaMalloc(&c.kv, 4 * nn * sizeof(uint32_t)));
+      if (!sp_alloc[s]) {
+        LCS_CUDA(cudaMalloc(&sp_alloc[s], (size_t)kSortedProps * nn * sizeof(uint64_t)));
+        sp_spare[s] = sp_alloc[s];
+      }
+      size_t sort_bytes = 0, scan_bytes = 0;
+      LCS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, c.kv, c.kv + n, c.kv + 2 * n, c.kv + 3 * n,
+                                               (int)n, 0, 32, stream));
+      LCS_CUDA(cub::DeviceScan::InclusiveScan(nullptr, scan_bytes, c.S, c.S + H + 1, MaxI64(), (int)(H + 1),
+                                              stream));
+      c.temp_bytes = std::max<size_t>(std::max(sort_bytes, scan_bytes), 1);
+      LCS_CUDA(cudaMalloc(&c.temp, c.temp_bytes));
+      c.ratio = ratio;
+    }
+    c.cg = cg;
+    c.H = H;
+    cudaEvent_t span = nullptr;  // the whole index, device-timed when profiling
+    if (prof && !capturing) {
+      span = get_event();
+      cudaEventRecord(span, stream);
+    }
+    int end_bit = 1;
+    while (end_bit < 32 && ((int64_t)1 << end_bit) <= H) end_bit++;
+    const int pos = stage_ == 1 ? LCS_PROP_X : LCS_PROP_X2;
+    const unsigned int nb = blocks_for(n, 256, 148 * 16);
+    uint32_t *kin = c.kv, *kout = c.kv + n, *vin = c.kv + 2 * n, *vout = c.kv + 3 * n;
+    LCS_TRY(launch("cell_hash", k_cell_hash, dim3(nb), dim3(256), 0, (const double*)sp[s].p[pos],
+                   (const double*)sp[s].p[pos + 1], (const double*)sp[s].p[pos + 2], n, cg, kin, vin));
+    // a stable LSD radix sort of (hash, index): equal hashes keep their order
+    LCS_TRY(timed("radix_sort", [&] {
+      size_t tb = c.temp_bytes;
+      return cub::DeviceRadixSort::SortPairs(c.temp, tb, kin, kout, vin, vout, (int)n, 0, end_bit, stream);
+    }));
+    // every property (16 FP64 ones and the ids, back to back from p[0]) in
+    // the sorted order into the spare block, which becomes the species' block
+    uint64_t* block = (uint64_t*)sp[s].p[0];
+    LCS_TRY(launch("permute", k_permute_props, dim3(nb), dim3(256), 0, (const uint64_t*)block, (const uint32_t*)vout,
+                   n, sp_spare[s]));
+    for (int q = 0; q < 16; q++) sp[s].p[q] = (double*)sp_spare[s] + (size_t)q * n;
+    sp_spare[s] = block;
+    LCS_TRY(launch("species_base", k_set_species_base, dim3(1), dim3(1), 0, dctx, s, sp[s].p[0]));
+    LCS_CUDA(cudaMemsetAsync(c.S, 0, (size_t)(H + 1) * sizeof(int64_t), stream));
+    LCS_TRY(launch("hash_runs", k_hash_runs, dim3(nb), dim3(256), 0, (const uint32_t*)kout, n, H, c.hashes, c.S));
+    LCS_TRY(timed("run_scan", [&] {
+      size_t tb = c.temp_bytes;
+      return cub::DeviceScan::InclusiveScan(c.temp, tb, c.S, c.S + H + 1, MaxI64(), (int)(H + 1), stream);
+    }));
+    LCS_TRY(launch("starts_stops", k_starts_stops, dim3(blocks_for(H, 256, 148 * 16)), dim3(256), 0,
+                   (const int64_t*)(c.S + H + 1), H, c.starts, c.starts + H));
+    if (span) {
+      cudaEvent_t b = get_event();
+      cudaEventRecord(b, stream);
+      recs.push_back({"makeindex", span, b});
+    }
+    LCS_TRY(collect_profile());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    c.built = true;
+    return LCS_OK;
+  }
+  int particles_cellindex(int s, int64_t* hashes, int64_t* starts, int64_t* stops) override {
+    LCS_TRY(check_species(s));
+    if (!ci[s].built) return fail(LCS_ESTATE, "no cell index built for species %d", s);
+    const CellIndex& c = ci[s];
+    if (hashes) LCS_TRY(copy(hashes, c.hashes, (size_t)sp[s].n * 8, cudaMemcpyDeviceToHost));
+    if (starts) LCS_TRY(copy(starts, c.starts, (size_t)c.H * 8, cudaMemcpyDeviceToHost));
+    if (stops) LCS_TRY(copy(stops, c.starts + c.H, (size_t)c.H * 8, cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
   int particles_timestep(double* dt) override {
     LCS_TRY(read_ctx());
     if (dt) *dt = (cfg.mode == LCS_MODE_FLOW_PARTICLE && cfg.n_species > 0) ? hctx->dt_particles : cfg.dtmax;
@@ -1429,7 +1572,7 @@ class Engine : public EngineBase {
     LCS_TRY(fill(kSetUs, false, g.h, 1));
     if (sp[s].n > 0)
       LCS_TRY(launch("particles_init_velocity", k_particles_init_velocity<T>, dim3((unsigned)((sp[s].n + 255) / 256)),
-                     dim3(256), 0, (const Ctx*)dctx, g, sp[s], pc));
+                     dim3(256), 0, (const Ctx*)dctx, g, s, sp[s], pc));
     LCS_CUDA(cudaStreamSynchronize(stream));
     return LCS_OK;
   }

@@ -1294,11 +1294,21 @@ struct PartCoef {
 // modes: bit0 boundary!, bit1 motion!, bit2 update!.  With motion and update
 // together dudt stays in registers.  `use_stage_dt` reads dtrk from the
 // device context (graph replays), else dt_arg.
+// The property arrays of species s are read from the device context (the
+// species' block moves when a cell index reorders it), so graphs captured
+// before the move stay valid.
+__device__ __forceinline__ void species_arrays(const Ctx* __restrict__ ctx, int s, SpeciesDev& sp) {
+  double* b = ctx->sp_base[s];
+#pragma unroll
+  for (int q = 0; q < 16; q++) sp.p[q] = b + q * sp.n;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_particles(const Ctx* __restrict__ ctx, Grid g, SpeciesDev sp, PartCoef pc,
-                                                   int stage, int modes, int use_stage_dt, double dt_arg) {
+__global__ void __launch_bounds__(256) k_particles(const Ctx* __restrict__ ctx, Grid g, int s, SpeciesDev sp,
+                                                   PartCoef pc, int stage, int modes, int use_stage_dt, double dt_arg) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= sp.n) return;
+  species_arrays(ctx, s, sp);
   const double L = kDomainLength;
   // stage 1: xss / xss2 partner; stage 2: xss2 / xss partner (boundary.jl:22-26)
   double* X[3] = {sp.p[stage == 1 ? 0 : 3], sp.p[stage == 1 ? 1 : 4], sp.p[stage == 1 ? 2 : 5]};
@@ -1372,9 +1382,10 @@ __global__ void __launch_bounds__(256) k_particles(const Ctx* __restrict__ ctx, 
 
 // New init kind: particle velocity = trilinear interpolation of Us.
 template <typename T>
-__global__ void k_particles_init_velocity(const Ctx* __restrict__ ctx, Grid g, SpeciesDev sp, PartCoef pc) {
+__global__ void k_particles_init_velocity(const Ctx* __restrict__ ctx, Grid g, int s, SpeciesDev sp, PartCoef pc) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= sp.n) return;
+  species_arrays(ctx, s, sp);
   const double x = sp.p[0][p], y = sp.p[1][p], z = sp.p[2][p];
   sp.p[6][p] = interp<T>((const T*)ctx->vel[kSetUs][0], g, xmapping(x, y, z, pc.dx, pc.dy, pc.dz));
   sp.p[7][p] = interp<T>((const T*)ctx->vel[kSetUs][1], g, ymapping(x, y, z, pc.dx, pc.dy, pc.dz));
@@ -1435,6 +1446,7 @@ __global__ void k_convert_out(double* __restrict__ dst, const T* __restrict__ sr
 // --------------------------------------------------------------------------
 __global__ void k_set_stage_dt(Ctx* ctx, int stage) { ctx->scal[0] = stage == 1 ? 0.5 * ctx->dt : ctx->dt; }
 __global__ void k_set_scalar(double* dst, double v) { *dst = v; }
+__global__ void k_set_species_base(Ctx* ctx, int s, double* base) { ctx->sp_base[s] = base; }
 __global__ void k_step_begin(Ctx* ctx) {
   ctx->cur.p = __longlong_as_double(0x7ff8000000000000LL);
   ctx->cur.e10 = __longlong_as_double(0x7ff8000000000000LL);

@@ -203,6 +203,8 @@ PROTOTYPES = {
     "lcs_flow_timestep_noalloc": (C.c_int, [_P, _P, _P, C.POINTER(C.c_int32), C.c_int32, C.c_double, C.c_double,
                                             C.c_double, _P, _P]),
     "lcs_flow_stat": (C.c_int, [_P, C.POINTER(FlowStat)]),
+    "lcs_particles_makeindex": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
+    "lcs_particles_cellindex": (C.c_int, [_P, C.c_int32, _I64, _I64, _I64]),
     "lcs_step_begin": (C.c_int, [_P, C.c_int32]),
     "lcs_step_poll": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "lcs_step_finish": (C.c_int, [_P, C.POINTER(Log)]),

@@ -174,6 +174,20 @@ class Engine:
         self._check(self.lib.lcs_step(self.handle, nsteps, arr if logs else None))
         return [arr[q].as_dict() for q in range(nsteps)] if logs else None
 
+    def particles_makeindex(self, species: int, stage: int, grid_ratio: int):
+        """`Particles.makeindex!` (src/particles/makeindex.jl:29-67): sorts the species by cell hash."""
+        self._check(self.lib.lcs_particles_makeindex(self.handle, species, stage, grid_ratio))
+
+    def particles_cellindex(self, species: int, grid_ratio: int):
+        """(hashes, starts, stops) of the last makeindex of the species."""
+        nc = [d // grid_ratio for d in self.n]
+        H = (nc[0] + 2) * (nc[1] + 2) * (nc[2] + 2)
+        n = int(self.cfg.species[species].nvalid)
+        hashes, starts, stops = np.empty(n, np.int64), np.empty(H, np.int64), np.empty(H, np.int64)
+        p = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))  # noqa: E731
+        self._check(self.lib.lcs_particles_cellindex(self.handle, species, p(hashes), p(starts), p(stops)))
+        return hashes, starts, stops
+
     def flow_stat(self) -> dict:
         """`Flows.stat` (src/flows/stat.jl:66-153) computed on the device."""
         st = _abi.FlowStat()

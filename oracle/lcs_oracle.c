@@ -48,6 +48,8 @@ typedef struct {
   int64_t n;
   double* p[LCS_NPROP];
   int64_t* ids;
+  int64_t *ci_hashes, *ci_starts, *ci_stops; /* the last cell index (makeindex.jl:29-67) */
+  int64_t ci_H;
 } species_t;
 
 struct lcs_handle {
@@ -900,6 +902,9 @@ void lcs_destroy(lcs_handle* h) {
   for (int s = 0; s < h->cfg.n_species; s++) {
     for (int q = 0; q < LCS_NPROP; q++) free(h->sp[s].p[q]);
     free(h->sp[s].ids);
+    free(h->sp[s].ci_hashes);
+    free(h->sp[s].ci_starts);
+    free(h->sp[s].ci_stops);
   }
   free(h->async_logs);
   free(h);
@@ -1208,6 +1213,102 @@ int lcs_flow_forcing(lcs_handle* h, double dtrk, double* p, double* e10) {
   else if (h->cfg.forcing == LCS_FORCING_RC_ENERGY) pp = forcing_rcf(h, dtrk, &ee);
   if (p) *p = pp;
   if (e10) *e10 = ee;
+  return LCS_OK;
+}
+/* `Particles.makeindex!` (src/particles/makeindex.jl:29-67).  Cell index
+ * ci = unsafe_floor(Int32, (x - x0) / dxc) + 1 with dxc = spacing * grid_ratio
+ * (particles/config.jl:60), hash = Utils.sub2ind over the axes 0:nc+1
+ * (src/utils/hasher.jl:15-38), a stable sort of the particles by hash
+ * (makeindex.jl:54-58: sortperm! then sortbyperm! of hashes and every
+ * property), then the binary searches of src/utils/fast.jl:8-40 for starts and
+ * stops of every hash 1..(nc+2)^3 (makeindex.jl:60-66). */
+typedef struct { int64_t h, i; } hash_idx;
+static int cmp_hash_idx(const void* a, const void* b) {
+  const hash_idx *x = (const hash_idx*)a, *y = (const hash_idx*)b;
+  if (x->h != y->h) return x->h < y->h ? -1 : 1;
+  return x->i < y->i ? -1 : (x->i > y->i);  /* equal hashes keep their order: stable */
+}
+static int64_t sorted_first(const int64_t* a, int64_t n, int64_t x) { /* fast.jl:8-24 */
+  int64_t lo = 1, len = n;
+  while (len != 0) {
+    int64_t half = len >> 1, m = lo + half;
+    if (a[m - 1] < x) { lo = m + 1; len -= half + 1; }
+    else len = half;
+  }
+  return lo;
+}
+static int64_t sorted_last(const int64_t* a, int64_t n, int64_t x) { /* fast.jl:26-40 */
+  int64_t lo = 0, hi = n + 1;
+  while (lo < hi - 1) {
+    int64_t m = lo + ((hi - lo) >> 1);
+    if (x < a[m - 1]) hi = m;
+    else lo = m;
+  }
+  return lo;
+}
+int lcs_particles_makeindex(lcs_handle* h, int32_t s, int32_t stage, int32_t ratio) {
+  int rc = check_species(h, s);
+  if (rc) return rc;
+  if (stage != 1 && stage != 2) return fail(h, LCS_EINVAL, "stage must be 1 or 2");
+  const grid_t* g = &h->g;
+  if (ratio < 1 || g->n[0] % ratio || g->n[1] % ratio || g->n[2] % ratio)
+    return fail(h, LCS_EINVAL, "grid_ratio must be positive and divide the grid dims");
+  species_t* sp = &h->sp[s];
+  const int64_t n = sp->n;
+  int nc[3];
+  double dxc[3];
+  int64_t H = 1;
+  for (int a = 0; a < 3; a++) {
+    nc[a] = g->n[a] / ratio;
+    dxc[a] = spacing(g, a) * ratio;
+    H *= nc[a] + 2;
+  }
+  if (H > (int64_t)UINT32_MAX) return fail(h, LCS_EINVAL, "cell index too large");
+  const int pos = stage == 1 ? LCS_PROP_X : LCS_PROP_X2;
+  hash_idx* hi = (hash_idx*)malloc((size_t)n * sizeof *hi);
+  double* tmp = (double*)malloc((size_t)n * sizeof *tmp);
+  free(sp->ci_hashes);
+  free(sp->ci_starts);
+  free(sp->ci_stops);
+  sp->ci_hashes = (int64_t*)malloc((size_t)n * sizeof(int64_t));
+  sp->ci_starts = (int64_t*)malloc((size_t)H * sizeof(int64_t));
+  sp->ci_stops = (int64_t*)malloc((size_t)H * sizeof(int64_t));
+  sp->ci_H = H;
+  for (int64_t i = 0; i < n; i++) {
+    int64_t hash = 1, stride = 1;
+    for (int a = 0; a < 3; a++) {
+      int ci = (int)floor((sp->p[pos + a][i] - DOMAIN_ORIGIN) / dxc[a]) + 1;
+      hash += (int64_t)ci * stride; /* offset from the axis start 0 */
+      stride *= nc[a] + 2;
+    }
+    hi[i].h = hash;
+    hi[i].i = i;
+  }
+  qsort(hi, (size_t)n, sizeof *hi, cmp_hash_idx);
+  for (int q = 0; q < LCS_NPROP; q++) {
+    for (int64_t i = 0; i < n; i++) tmp[i] = sp->p[q][hi[i].i];
+    memcpy(sp->p[q], tmp, (size_t)n * sizeof(double));
+  }
+  int64_t* itmp = (int64_t*)tmp;
+  for (int64_t i = 0; i < n; i++) itmp[i] = sp->ids[hi[i].i];
+  memcpy(sp->ids, itmp, (size_t)n * sizeof(int64_t));
+  for (int64_t i = 0; i < n; i++) sp->ci_hashes[i] = hi[i].h;
+  for (int64_t x = 1; x <= H; x++) {
+    sp->ci_starts[x - 1] = sorted_first(sp->ci_hashes, n, x);
+    sp->ci_stops[x - 1] = sorted_last(sp->ci_hashes, n, x);
+  }
+  free(hi);
+  free(tmp);
+  return LCS_OK;
+}
+int lcs_particles_cellindex(lcs_handle* h, int32_t s, int64_t* hashes, int64_t* starts, int64_t* stops) {
+  int rc = check_species(h, s);
+  if (rc) return rc;
+  const species_t* sp = &h->sp[s];
+  if (!sp->ci_hashes) return fail(h, LCS_ESTATE, "no cell index built for species %d", s);
+  if (hashes) memcpy(hashes, sp->ci_hashes, (size_t)sp->n * sizeof(int64_t));
+  if (starts) memcpy(starts, sp->ci_starts, (size_t)sp->ci_H * sizeof(int64_t));
+  if (stops) memcpy(stops, sp->ci_stops, (size_t)sp->ci_H * sizeof(int64_t));
   return LCS_OK;
 }
 int lcs_particles_boundary(lcs_handle* h, int32_t s, int32_t stage) {

@@ -664,6 +664,20 @@ def run_makeindex(args):
     eng.profile(False)
     hashes, starts, stops = eng.particles_cellindex(0, ratio)
     ok = bool(np.all(np.diff(hashes) >= 0)) and int(np.sum(stops - starts + 1)) == hashes.size
+    # Particles.stat of every species with the reference's production settings
+    # (cfgs/N1024-1.lcs-yaml: grid_ratio 4, 16 bins from 1.25e-4, search 2
+    # cells, contact 0.01, 64 directions up to k = 768), device-timed per kernel
+    tau_eta = eng.flow_stat()["tau_eta"]
+    for s in range(nsp):  # warm-up (scratch allocation)
+        eng.particles_stat(s, tau_eta, max_wavenumber=768)
+    eng.profile(True)
+    eng.profile_reset()
+    t0 = time.perf_counter()
+    for s in range(nsp):
+        eng.particles_stat(s, tau_eta, max_wavenumber=768)
+    stat_wall_ms = (time.perf_counter() - t0) * 1e3
+    stat_ms = {k: v[0] for k, v in eng.profile_totals().items()}
+    eng.profile(False)
     launches = eng.launch_count()
     eng.close()
     peak, peak_src = hbm_peak()
@@ -681,6 +695,9 @@ def run_makeindex(args):
         "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
                      "peak_source": peak_src, "algorithmic_bytes": algo},
         "invariants_ok": ok, "gpu_launches_total": launches,
+        "particle_stat": {"wall_ms": stat_wall_ms, "device_ms": stat_ms,
+                          "note": "Particles.stat of all 3 species (Summary, makeindex!, rdf, spectrum 19 shells x "
+                                  "64 directions)"},
         "timing": "CUDA events on the engine stream around each index (profiling spans)",
     }
     if not args.no_cpu_baseline:

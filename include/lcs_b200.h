@@ -247,6 +247,53 @@ LCS_API int lcs_particles_makeindex(lcs_handle* h, int32_t species, int32_t stag
  * stops[(nc+2)^3] (Int64, as LCS.IP); NULL pointers are skipped. */
 LCS_API int lcs_particles_cellindex(lcs_handle* h, int32_t species, int64_t* hashes, int64_t* starts, int64_t* stops);
 
+/* `Particles.stat` (src/particles/stat.jl:113-151) of species s: Summary
+ * (mean, max, min; src/stat.jl:20-22) of xss, uss and diams, taup of the mean
+ * diameter (config.jl:41), St = taup / tau_eta (tau_eta of the flow's stat,
+ * lcs_flow_stat), then makeindex! on xss (the species is reordered, as in the
+ * reference), the radial distribution function of rdf_assume_ci
+ * (src/particles/rdf.jl:1-103) and the number-density spectrum
+ * (src/particles/spectrum.jl:11-78).  The configuration mirrors Cell, RDF and
+ * Spectrum (src/particles/config.jl:51-94). */
+#define LCS_RDF_MAX_BINS 1024
+#define LCS_SPECTRUM_MAX_SHELLS 19 /* the WAVENUMBERS table, spectrum.jl:1 */
+#define LCS_SPECTRUM_MAX_SAMPLES 1024
+typedef struct lcs_particle_stat_config {
+  int32_t grid_ratio;        /* Cell.grid_ratio */
+  int32_t bin_size;          /* RDF.bin_size: number of bins, 1..LCS_RDF_MAX_BINS */
+  int32_t search_cell_size;  /* RDF.search_cell_size */
+  int32_t max_wavenumber;    /* Spectrum.max_wavenumber */
+  int32_t nsamples;          /* Spectrum.nsamples: directions, 2..LCS_SPECTRUM_MAX_SAMPLES */
+  int32_t pad_;
+  double contact_tolerance;  /* RDF.contact_tolerance */
+  double min_radius;         /* RDF.min_radius */
+} lcs_particle_stat_config;
+typedef struct lcs_summary {
+  double mean, max, min;
+} lcs_summary;
+typedef struct lcs_particle_stats {
+  lcs_summary x, y, z, u, v, w, diam;
+  double taup, St;
+  /* RDFStat (stat.jl:30-38): edges[nbins+1] are logrange(min_radius,
+   * search_cell_size * min spacing, nbins + 1) */
+  double gr_contact;
+  int64_t npairs_contact;
+  int32_t nbins, nshells;
+  double edges[LCS_RDF_MAX_BINS + 1];
+  double gr[LCS_RDF_MAX_BINS];
+  int64_t npairs[LCS_RDF_MAX_BINS];
+  /* SpectrumStat (stat.jl:10-15) */
+  double wavenumbers[LCS_SPECTRUM_MAX_SHELLS];
+  double Enp[LCS_SPECTRUM_MAX_SHELLS];
+} lcs_particle_stats;
+LCS_API int lcs_particles_stat(lcs_handle* h, int32_t species, const lcs_particle_stat_config* cfg, double tau_eta,
+                               lcs_particle_stats* out);
+/* `Particles.density` (src/particles/stat.jl:176-215): makeindex! on xss
+ * (reorders the species), then per particle the cubic-spline SPH sum over the
+ * 27 neighbouring cells with h = min spacing; densities[nvalid] in the new
+ * device order (0 for a particle outside the cell domain). */
+LCS_API int lcs_particles_density(lcs_handle* h, int32_t species, int32_t grid_ratio, double* densities);
+
 /* ---- asynchronous steps (no reference counterpart) ----------------------
  * For hosts that drive many handles at once (the batching and serving forms
  * below, or a Julia task per handle).  lcs_step_begin enqueues nsteps

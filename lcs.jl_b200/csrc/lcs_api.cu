@@ -168,6 +168,15 @@ int lcs_particles_cellindex(lcs_handle* h, int32_t s, int64_t* hashes, int64_t* 
   H(h);
   return h->e->particles_cellindex(s, hashes, starts, stops);
 }
+int lcs_particles_stat(lcs_handle* h, int32_t s, const lcs_particle_stat_config* pc, double tau_eta,
+                       lcs_particle_stats* out) {
+  H(h);
+  return h->e->particles_stat(s, pc, tau_eta, out);
+}
+int lcs_particles_density(lcs_handle* h, int32_t s, int32_t ratio, double* densities) {
+  H(h);
+  return h->e->particles_density(s, ratio, densities);
+}
 int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, double share) {
   H(h);
   return h->e->set_tuning(rw_rows, zchunk, share);

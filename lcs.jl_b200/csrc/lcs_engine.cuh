@@ -26,6 +26,10 @@
 #include "lcs_hsmac_tma.cuh"
 #include "lcs_hsmac_rw.cuh"
 #include "lcs_makeindex.cuh"
+#include "lcs_pstat.cuh"
+
+// bin edges of logrange(a, b, len) in extended precision (lcs_hostmath.cpp)
+extern "C" void lcs_logrange(double a, double b, int len, double* out);
 
 namespace lcs {
 
@@ -170,6 +174,9 @@ class Engine : public EngineBase {
   // first index): the permutation writes the spare block and the two swap.
   uint64_t* sp_alloc[LCS_MAX_SPECIES] = {};  // owned (cudaMalloc)
   uint64_t* sp_spare[LCS_MAX_SPECIES] = {};  // the block not in use (sp_alloc or the one in the pool)
+  // scratch of the particle statistics (grown on demand)
+  char* pbuf = nullptr;
+  size_t pbuf_bytes = 0;
   bool uploaded_flow = false;
   int64_t launches = 0;
   // profiling
@@ -207,6 +214,7 @@ class Engine : public EngineBase {
     if (hlogs) cudaFreeHost(hlogs);
     for (auto& c : ci) free_index(c);
     for (auto* a : sp_alloc) cudaFree(a);
+    cudaFree(pbuf);
     if (async_ev) cudaEventDestroy(async_ev);
     if (pool) cudaFree(pool);
     if (stream) cudaStreamDestroy(stream);
@@ -1538,6 +1546,156 @@ class Engine : public EngineBase {
     if (hashes) LCS_TRY(copy(hashes, c.hashes, (size_t)sp[s].n * 8, cudaMemcpyDeviceToHost));
     if (starts) LCS_TRY(copy(starts, c.starts, (size_t)c.H * 8, cudaMemcpyDeviceToHost));
     if (stops) LCS_TRY(copy(stops, c.starts + c.H, (size_t)c.H * 8, cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  int ensure_pbuf(size_t bytes) {
+    if (bytes <= pbuf_bytes) return LCS_OK;
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    cudaFree(pbuf);
+    pbuf = nullptr;
+    pbuf_bytes = 0;
+    LCS_CUDA(cudaMalloc(&pbuf, bytes));
+    pbuf_bytes = bytes;
+    return LCS_OK;
+  }
+  // `Particles.stat` (src/particles/stat.jl:113-151)
+  int particles_stat(int s, const lcs_particle_stat_config* pc, double tau_eta, lcs_particle_stats* out) override {
+    LCS_TRY(check_species(s));
+    if (!pc || !out) return fail(LCS_EINVAL, "null config or output");
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    const int nbins = pc->bin_size, ns = pc->nsamples;
+    if (nbins < 1 || nbins > LCS_RDF_MAX_BINS) return fail(LCS_EINVAL, "bin_size must be 1..%d", LCS_RDF_MAX_BINS);
+    if (ns < 2 || ns > LCS_SPECTRUM_MAX_SAMPLES) return fail(LCS_EINVAL, "nsamples must be 2..%d", LCS_SPECTRUM_MAX_SAMPLES);
+    if (pc->search_cell_size < 0 || pc->search_cell_size > 64) return fail(LCS_EINVAL, "search_cell_size must be 0..64");
+    if (!(pc->min_radius > 0.0)) return fail(LCS_EINVAL, "min_radius must be positive");
+    const int64_t n = sp[s].n;
+    const double* P[7] = {sp[s].p[LCS_PROP_X], sp[s].p[LCS_PROP_Y], sp[s].p[LCS_PROP_Z], sp[s].p[LCS_PROP_U],
+                          sp[s].p[LCS_PROP_V], sp[s].p[LCS_PROP_W], sp[s].p[LCS_PROP_DIAM]};
+    // Summary of xss, uss, diams (stat.jl:131-139)
+    const unsigned int nbs = blocks_for(n, 256, 148 * 4);
+    LCS_TRY(launch("psummary", k_psummary, dim3(nbs), dim3(256), 0, P[0], P[1], P[2], P[3], P[4], P[5], P[6], n,
+                   partials));
+    LCS_TRY(launch("psummary_final", k_psummary_final, dim3(1), dim3(256), 0, (const double*)partials, (int)nbs, stage));
+    double v[kPSumVals];
+    LCS_TRY(copy(v, stage, sizeof v, cudaMemcpyDeviceToHost));
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    lcs_summary* S[7] = {&out->x, &out->y, &out->z, &out->u, &out->v, &out->w, &out->diam};
+    for (int q = 0; q < 7; q++) {
+      S[q]->mean = v[3 * q] / (double)n;
+      S[q]->max = v[3 * q + 1];
+      S[q]->min = v[3 * q + 2];
+    }
+    const double Re = cfg.U0 * cfg.L0 / cfg.NU;
+    const double dm = out->diam.mean;
+    out->taup = 1.0 / 18.0 * cfg.species[s].density_ratio * Re * (dm * dm);  // config.jl:41
+    out->St = out->taup / tau_eta;
+    LCS_TRY(particles_makeindex(s, 1, pc->grid_ratio));
+    const CellIndex& c = ci[s];
+    // rdf_assume_ci (rdf.jl:1-103)
+    const double hmin = std::min(kDomainLength / g.n[0], std::min(kDomainLength / g.n[1], kDomainLength / g.n[2]));
+    const double rmax = pc->search_cell_size * hmin;
+    out->nbins = nbins;
+    lcs_logrange(pc->min_radius, rmax, nbins + 1, out->edges);
+    const size_t need = std::max<size_t>((size_t)(nbins + 1) * 16, 0);
+    const int nshells = spectrum_shells(pc->max_wavenumber);
+    const int npairs = nshells * ns;
+    const unsigned int nbx = 148 * 2;
+    const size_t spec_bytes = (size_t)npairs * 3 * 8 + (size_t)nbx * npairs * 2 * 8 + (size_t)npairs * 2 * 8;
+    LCS_TRY(ensure_pbuf(need + spec_bytes + 64));
+    double* d_edges = (double*)pbuf;
+    unsigned long long* d_counts = (unsigned long long*)(pbuf + (size_t)(nbins + 1) * 8);
+    LCS_TRY(copy(d_edges, out->edges, (size_t)(nbins + 1) * 8, cudaMemcpyHostToDevice));
+    LCS_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)(nbins + 1) * 8, stream));
+    const size_t rdf_smem = (size_t)(nbins + 1) * 16;
+    LCS_TRY(launch("rdf", k_rdf, dim3(blocks_for(n, 256, 148 * 8)), dim3(256), rdf_smem, (const double*)sp[s].p[0],
+                   (const double*)sp[s].p[1], (const double*)sp[s].p[2], (const int64_t*)(sp[s].p[0] + 16 * n),
+                   (const int64_t*)c.hashes, (const int64_t*)c.starts, (const int64_t*)(c.starts + c.H), n, c.cg,
+                   pc->search_cell_size, (const double*)d_edges, nbins, dm, pc->contact_tolerance, d_counts));
+    std::vector<unsigned long long> counts(nbins + 1);
+    LCS_TRY(copy(counts.data(), d_counts, (size_t)(nbins + 1) * 8, cudaMemcpyDeviceToHost));
+    // the spectrum (spectrum.jl:11-78)
+    std::vector<double> kvec((size_t)npairs * 3 + 1), sums((size_t)npairs * 2 + 1);
+    out->nshells = nshells;
+    spectrum_directions(nshells, ns, kvec.data(), out->wavenumbers);
+    if (npairs > 0) {
+      double* d_k = (double*)(pbuf + need);
+      double* d_part = d_k + (size_t)npairs * 3;
+      double* d_sums = d_part + (size_t)nbx * npairs * 2;
+      LCS_TRY(copy(d_k, kvec.data(), (size_t)npairs * 3 * 8, cudaMemcpyHostToDevice));
+      const unsigned int nby = (unsigned)((npairs + 256 * kSpecPairs - 1) / (256 * kSpecPairs));
+      LCS_TRY(launch("spectrum", k_spectrum, dim3(nbx, nby), dim3(256), 0, (const double*)sp[s].p[0],
+                     (const double*)sp[s].p[1], (const double*)sp[s].p[2], n, (const double*)d_k, npairs, d_part));
+      LCS_TRY(launch("spectrum_final", k_spectrum_final, dim3((unsigned)((2 * npairs + 255) / 256)), dim3(256), 0,
+                     (const double*)d_part, (int)nbx, npairs, d_sums));
+      LCS_TRY(copy(sums.data(), d_sums, (size_t)npairs * 2 * 8, cudaMemcpyDeviceToHost));
+    }
+    LCS_TRY(collect_profile());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    // host finish: rdf.jl:80-100, spectrum.jl:63-75, in the reference's order
+    const double L = kDomainLength;
+    const double vol = L * L * L;
+    const double rho0 = (double)(n * (n - 1) / 2) / vol;
+    for (int k = 0; k < nbins; k++) {
+      const double e0 = out->edges[k], e1 = out->edges[k + 1];
+      const double vol_shell = (4.0 / 3.0) * M_PI * (e1 * e1 * e1 - e0 * e0 * e0);
+      out->npairs[k] = (int64_t)counts[k];
+      out->gr[k] = ((double)counts[k] / vol_shell) / rho0;
+    }
+    out->npairs_contact = (int64_t)counts[nbins];
+    const double vol_contact = (4.0 / 3.0) * M_PI * (dm * dm * dm) * 6.0 * pc->contact_tolerance;
+    out->gr_contact = ((double)counts[nbins] / vol_contact) / rho0;
+    const double N2 = (double)(n * n);
+    for (int b = 0; b < nshells; b++) {
+      double phi = 0.0;
+      for (int i = 0; i < ns; i++) {
+        const double cc = sums[2 * (b * ns + i)], ss = sums[2 * (b * ns + i) + 1];
+        phi += (cc * cc + ss * ss) / N2 - 1.0 / (double)n;
+      }
+      const double kk = out->wavenumbers[b];
+      out->Enp[b] = phi / ns * 4.0 * M_PI * (kk * kk);
+    }
+    return LCS_OK;
+  }
+  static int spectrum_shells(int max_wavenumber) {
+    int c = 0;
+    while (c < LCS_SPECTRUM_MAX_SHELLS && kWavenumbers[c] <= max_wavenumber) c++;
+    return c;  // Utils.searchsortedlast(WAVENUMBERS, max_wavenumber)
+  }
+  // k = kk .* _fibonacci_direction(i, nsamples) (spectrum.jl:3-9, 37-38)
+  static void spectrum_directions(int nshells, int ns, double* kvec, double* wavenumbers) {
+    const double phi = M_PI * (3.0 - std::sqrt(5.0));
+    for (int b = 0; b < nshells; b++) {
+      const double kk = kWavenumbers[b];
+      wavenumbers[b] = kk;
+      for (int i = 0; i < ns; i++) {
+        const double y = 1.0 - ((double)i / (double)(ns - 1)) * 2.0;
+        const double radius = std::sqrt(1.0 - y * y);
+        const double theta = phi * i;
+        double* k = kvec + 3 * ((size_t)b * ns + i);
+        k[0] = kk * (std::cos(theta) * radius);
+        k[1] = kk * y;
+        k[2] = kk * (std::sin(theta) * radius);
+      }
+    }
+  }
+  static constexpr int kWavenumbers[LCS_SPECTRUM_MAX_SHELLS] = {1,  2,  3,   4,   6,   8,   12,  16,  24, 32,
+                                                                48, 64, 96, 128, 192, 256, 384, 512, 768};
+  // `Particles.density` (src/particles/stat.jl:176-215)
+  int particles_density(int s, int ratio, double* densities) override {
+    LCS_TRY(check_species(s));
+    if (!densities) return fail(LCS_EINVAL, "null output");
+    LCS_TRY(particles_makeindex(s, 1, ratio));
+    const CellIndex& c = ci[s];
+    const int64_t n = sp[s].n;
+    const double h = std::min(kDomainLength / g.n[0], std::min(kDomainLength / g.n[1], kDomainLength / g.n[2]));
+    const double factor = 1.0 / (M_PI * (h * h * h));
+    LCS_TRY(ensure_pbuf((size_t)n * 8));
+    LCS_TRY(launch("density", k_density, dim3(blocks_for(n, 256, 148 * 8)), dim3(256), 0, (const double*)sp[s].p[0],
+                   (const double*)sp[s].p[1], (const double*)sp[s].p[2], (const int64_t*)c.hashes,
+                   (const int64_t*)c.starts, (const int64_t*)(c.starts + c.H), n, c.cg, h, factor, (double*)pbuf));
+    LCS_TRY(copy(densities, pbuf, (size_t)n * 8, cudaMemcpyDeviceToHost));
+    LCS_TRY(collect_profile());
     LCS_CUDA(cudaStreamSynchronize(stream));
     return LCS_OK;
   }

@@ -128,6 +128,45 @@ class FlowStat(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+# ---- particle statistics (include/lcs_b200.h: lcs_particles_stat) -----------
+RDF_MAX_BINS = 1024
+SPECTRUM_MAX_SHELLS = 19
+SPECTRUM_MAX_SAMPLES = 1024
+
+
+class ParticleStatConfig(C.Structure):
+    """Cell, RDF and Spectrum of src/particles/config.jl:51-94."""
+    _fields_ = [("grid_ratio", C.c_int32), ("bin_size", C.c_int32), ("search_cell_size", C.c_int32),
+                ("max_wavenumber", C.c_int32), ("nsamples", C.c_int32), ("_pad", C.c_int32),
+                ("contact_tolerance", C.c_double), ("min_radius", C.c_double)]
+
+
+class Summary(C.Structure):
+    _fields_ = [("mean", C.c_double), ("max", C.c_double), ("min", C.c_double)]
+
+
+class ParticleStats(C.Structure):
+    _fields_ = [(f, Summary) for f in ("x", "y", "z", "u", "v", "w", "diam")] + [
+        ("taup", C.c_double), ("St", C.c_double), ("gr_contact", C.c_double), ("npairs_contact", C.c_int64),
+        ("nbins", C.c_int32), ("nshells", C.c_int32), ("edges", C.c_double * (RDF_MAX_BINS + 1)),
+        ("gr", C.c_double * RDF_MAX_BINS), ("npairs", C.c_int64 * RDF_MAX_BINS),
+        ("wavenumbers", C.c_double * SPECTRUM_MAX_SHELLS), ("Enp", C.c_double * SPECTRUM_MAX_SHELLS)]
+
+    def as_dict(self) -> dict:
+        """ParticleStat (src/particles/stat.jl:62-75) as nested dicts and numpy arrays."""
+        import numpy as np
+
+        nb, ns = self.nbins, self.nshells
+        out = {f: {"mean": getattr(self, f).mean, "max": getattr(self, f).max, "min": getattr(self, f).min}
+               for f in ("x", "y", "z", "u", "v", "w", "diam")}
+        out["taup"], out["St"] = self.taup, self.St
+        out["rdf"] = {"gr_contact": self.gr_contact, "npairs_contact": self.npairs_contact,
+                      "edges": np.array(self.edges[: nb + 1]), "gr": np.array(self.gr[:nb]),
+                      "npairs": np.array(self.npairs[:nb], dtype=np.int64)}
+        out["spectrum"] = {"wavenumbers": np.array(self.wavenumbers[:ns]), "Enp": np.array(self.Enp[:ns])}
+        return out
+
+
 # ---- batching and serving forms (include/lcs_b200.h) -----------------------
 MAX_ASYNC_STEPS = 4096
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
@@ -205,6 +244,9 @@ PROTOTYPES = {
     "lcs_flow_stat": (C.c_int, [_P, C.POINTER(FlowStat)]),
     "lcs_particles_makeindex": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
     "lcs_particles_cellindex": (C.c_int, [_P, C.c_int32, _I64, _I64, _I64]),
+    "lcs_particles_stat": (C.c_int, [_P, C.c_int32, C.POINTER(ParticleStatConfig), C.c_double,
+                                     C.POINTER(ParticleStats)]),
+    "lcs_particles_density": (C.c_int, [_P, C.c_int32, C.c_int32, _D]),
     "lcs_step_begin": (C.c_int, [_P, C.c_int32]),
     "lcs_step_poll": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "lcs_step_finish": (C.c_int, [_P, C.POINTER(Log)]),

@@ -188,6 +188,24 @@ class Engine:
         self._check(self.lib.lcs_particles_cellindex(self.handle, species, p(hashes), p(starts), p(stops)))
         return hashes, starts, stops
 
+    def particles_stat(self, species: int, tau_eta: float, grid_ratio: int = 4, bin_size: int = 16,
+                       search_cell_size: int = 2, contact_tolerance: float = 0.01, min_radius: float = 1.25e-4,
+                       max_wavenumber: int = 128, nsamples: int = 64) -> dict:
+        """`Particles.stat` (src/particles/stat.jl:113-151); reorders the species
+        by cell (makeindex!).  Defaults: the reference's cfgs/N1024-1.lcs-yaml."""
+        pc = _abi.ParticleStatConfig(grid_ratio=grid_ratio, bin_size=bin_size, search_cell_size=search_cell_size,
+                                     max_wavenumber=max_wavenumber, nsamples=nsamples,
+                                     contact_tolerance=contact_tolerance, min_radius=min_radius)
+        out = _abi.ParticleStats()
+        self._check(self.lib.lcs_particles_stat(self.handle, species, C.byref(pc), float(tau_eta), C.byref(out)))
+        return out.as_dict()
+
+    def particles_density(self, species: int, grid_ratio: int) -> np.ndarray:
+        """`Particles.density` (src/particles/stat.jl:176-215), in the new device order."""
+        out = np.empty(int(self.cfg.species[species].nvalid))
+        self._check(self.lib.lcs_particles_density(self.handle, species, grid_ratio, _dptr(out)))
+        return out
+
     def flow_stat(self) -> dict:
         """`Flows.stat` (src/flows/stat.jl:66-153) computed on the device."""
         st = _abi.FlowStat()

@@ -27,6 +27,7 @@
 #include "../include/lcs_b200.h"
 
 #include <math.h>
+#include <quadmath.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -37,6 +38,7 @@
 
 #define DOMAIN_LENGTH (2.0 * 3.14159265358979323846) /* src/LCS.jl:17 */
 #define DOMAIN_ORIGIN 0.0                            /* src/LCS.jl:16 */
+#define PI_F64 3.14159265358979323846                /* Float64(pi) */
 
 typedef struct {
   int n[3];  /* interior cells per axis */
@@ -1309,6 +1311,169 @@ int lcs_particles_cellindex(lcs_handle* h, int32_t s, int64_t* hashes, int64_t* 
   if (hashes) memcpy(hashes, sp->ci_hashes, (size_t)sp->n * sizeof(int64_t));
   if (starts) memcpy(starts, sp->ci_starts, (size_t)sp->ci_H * sizeof(int64_t));
   if (stops) memcpy(stops, sp->ci_stops, (size_t)sp->ci_H * sizeof(int64_t));
+  return LCS_OK;
+}
+/* ---- particle statistics (src/particles/stat.jl:113-215, rdf.jl, spectrum.jl) */
+/* logrange(a, b, len) (Julia Base.LogRange): endpoints exact, the interior
+ * exp((len - i) log a + (i - 1) log b) / (len - 1)) evaluated in binary128. */
+static void oracle_logrange(double a, double b, int len, double* out) {
+  out[0] = a;
+  for (int i = 2; i < len; i++) {
+    __float128 x = ((__float128)(len - i) * logq((__float128)a) + (__float128)(i - 1) * logq((__float128)b)) /
+                   (__float128)(len - 1);
+    out[i - 1] = (double)expq(x);
+  }
+  out[len - 1] = b;
+}
+static const int WAVENUMBERS[19] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768};
+/* Utils.decode (src/utils/hasher.jl:40-59): 0-based offsets from the axis start 0 */
+static void decode_cell(int64_t hash, const int nc[3], int c[3]) {
+  int64_t lin = hash - 1;
+  for (int a = 0; a < 3; a++) {
+    c[a] = (int)(lin % (nc[a] + 2));
+    lin /= nc[a] + 2;
+  }
+}
+static double norm3(double a, double b, double c) { return sqrt(a * a + b * b + c * c); } /* fast.jl:43-47 */
+int lcs_particles_stat(lcs_handle* h, int32_t s, const lcs_particle_stat_config* pc, double tau_eta,
+                       lcs_particle_stats* out) {
+  int rc = check_species(h, s);
+  if (rc) return rc;
+  if (!pc || !out) return fail(h, LCS_EINVAL, "null config or output");
+  const int nbins = pc->bin_size, ns = pc->nsamples;
+  if (nbins < 1 || nbins > LCS_RDF_MAX_BINS) return fail(h, LCS_EINVAL, "bad bin_size");
+  if (ns < 2 || ns > LCS_SPECTRUM_MAX_SAMPLES) return fail(h, LCS_EINVAL, "bad nsamples");
+  if (pc->search_cell_size < 0 || pc->search_cell_size > 64) return fail(h, LCS_EINVAL, "bad search_cell_size");
+  if (!(pc->min_radius > 0.0)) return fail(h, LCS_EINVAL, "bad min_radius");
+  species_t* sp = &h->sp[s];
+  const int64_t n = sp->n;
+  /* Summary (src/stat.jl:20-22): mean = sum / n, sequential sum */
+  const int props[7] = {LCS_PROP_X, LCS_PROP_Y, LCS_PROP_Z, LCS_PROP_U, LCS_PROP_V, LCS_PROP_W, LCS_PROP_DIAM};
+  lcs_summary* S[7] = {&out->x, &out->y, &out->z, &out->u, &out->v, &out->w, &out->diam};
+  for (int q = 0; q < 7; q++) {
+    const double* a = sp->p[props[q]];
+    double sum = 0.0, mx = -INFINITY, mn = INFINITY;
+    for (int64_t i = 0; i < n; i++) {
+      sum += a[i];
+      mx = fmax(mx, a[i]);
+      mn = fmin(mn, a[i]);
+    }
+    S[q]->mean = sum / (double)n;
+    S[q]->max = mx;
+    S[q]->min = mn;
+  }
+  const lcs_config* c = &h->cfg;
+  const double Re = c->U0 * c->L0 / c->NU;
+  const double dm = out->diam.mean;
+  out->taup = 1.0 / 18.0 * c->species[s].density_ratio * Re * (dm * dm); /* config.jl:41 */
+  out->St = out->taup / tau_eta;
+  rc = lcs_particles_makeindex(h, s, 1, pc->grid_ratio);
+  if (rc) return rc;
+  /* rdf_assume_ci (rdf.jl:1-103) */
+  const grid_t* g = &h->g;
+  int nc[3];
+  for (int a = 0; a < 3; a++) nc[a] = g->n[a] / pc->grid_ratio;
+  const double hmin = fmin(spacing(g, 0), fmin(spacing(g, 1), spacing(g, 2)));
+  const double rmax = pc->search_cell_size * hmin;
+  out->nbins = nbins;
+  oracle_logrange(pc->min_radius, rmax, nbins + 1, out->edges);
+  int64_t cnt[LCS_RDF_MAX_BINS] = {0}, contact = 0;
+  const double *X = sp->p[LCS_PROP_X], *Y = sp->p[LCS_PROP_Y], *Z = sp->p[LCS_PROP_Z];
+  const int ncell = pc->search_cell_size;
+  for (int64_t i1 = 0; i1 < n; i1++) {
+    int c1[3];
+    decode_cell(sp->ci_hashes[i1], nc, c1);
+    if (c1[0] < 1 || c1[0] > nc[0] || c1[1] < 1 || c1[1] > nc[1] || c1[2] < 1 || c1[2] > nc[2]) continue;
+    for (int di = -ncell; di <= ncell; di++)
+      for (int dj = -ncell; dj <= ncell; dj++)
+        for (int dk = -ncell; dk <= ncell; dk++) {
+          const int a = c1[0] + di, b = c1[1] + dj, cc = c1[2] + dk;
+          if (a < 0 || a > nc[0] + 1 || b < 0 || b > nc[1] + 1 || cc < 0 || cc > nc[2] + 1) continue;
+          const int64_t h2 = 1 + a + (int64_t)b * (nc[0] + 2) + (int64_t)cc * (nc[0] + 2) * (nc[1] + 2);
+          for (int64_t i2 = sp->ci_starts[h2 - 1]; i2 <= sp->ci_stops[h2 - 1]; i2++) {
+            if (!(sp->ids[i1] < sp->ids[i2 - 1])) continue;
+            const double d = norm3(X[i1] - X[i2 - 1], Y[i1] - Y[i2 - 1], Z[i1] - Z[i2 - 1]);
+            int k = 0; /* searchsortedfirst(edges, d) - 1, by a linear scan */
+            while (k < nbins + 1 && out->edges[k] < d) k++;
+            if (k >= 1 && k <= nbins) cnt[k - 1]++;
+            if (fabs(d / dm - 1.0) < pc->contact_tolerance) contact++;
+          }
+        }
+  }
+  const double L = DOMAIN_LENGTH;
+  const double rho0 = (double)(n * (n - 1) / 2) / (L * L * L); /* binomial(n, 2) / volume_g() */
+  for (int k = 0; k < nbins; k++) {
+    const double e0 = out->edges[k], e1 = out->edges[k + 1];
+    const double vol_shell = (4.0 / 3.0) * PI_F64 * (e1 * e1 * e1 - e0 * e0 * e0);
+    out->npairs[k] = cnt[k];
+    out->gr[k] = ((double)cnt[k] / vol_shell) / rho0;
+  }
+  out->npairs_contact = contact;
+  out->gr_contact = ((double)contact / ((4.0 / 3.0) * PI_F64 * (dm * dm * dm) * 6.0 * pc->contact_tolerance)) / rho0;
+  /* spectrum (spectrum.jl:11-78): sequential sums over the particles */
+  int nshells = 0;
+  while (nshells < 19 && WAVENUMBERS[nshells] <= pc->max_wavenumber) nshells++;
+  out->nshells = nshells;
+  const double phi0 = PI_F64 * (3.0 - sqrt(5.0));
+  for (int b = 0; b < nshells; b++) {
+    const double kk = WAVENUMBERS[b];
+    out->wavenumbers[b] = kk;
+    double phi = 0.0;
+    for (int i = 0; i < ns; i++) {
+      const double y = 1.0 - ((double)i / (double)(ns - 1)) * 2.0;
+      const double radius = sqrt(1.0 - y * y);
+      const double theta = phi0 * i;
+      const double kx = kk * (cos(theta) * radius), ky = kk * y, kz = kk * (sin(theta) * radius);
+      double cs = 0.0, sn = 0.0;
+      for (int64_t p = 0; p < n; p++) {
+        const double kd = kx * X[p] + ky * Y[p] + kz * Z[p];
+        cs += cos(kd);
+        sn += sin(kd);
+      }
+      phi += (cs * cs + sn * sn) / (double)(n * n) - 1.0 / (double)n;
+    }
+    out->Enp[b] = phi / ns * 4.0 * PI_F64 * (kk * kk);
+  }
+  return LCS_OK;
+}
+/* `Particles.density` (stat.jl:176-215) */
+int lcs_particles_density(lcs_handle* h, int32_t s, int32_t ratio, double* rho_out) {
+  int rc = lcs_particles_makeindex(h, s, 1, ratio);
+  if (rc) return rc;
+  if (!rho_out) return fail(h, LCS_EINVAL, "null output");
+  const species_t* sp = &h->sp[s];
+  const grid_t* g = &h->g;
+  int nc[3];
+  for (int a = 0; a < 3; a++) nc[a] = g->n[a] / ratio;
+  const double hh = fmin(spacing(g, 0), fmin(spacing(g, 1), spacing(g, 2)));
+  const double factor = 1.0 / (PI_F64 * (hh * hh * hh));
+  const double *X = sp->p[LCS_PROP_X], *Y = sp->p[LCS_PROP_Y], *Z = sp->p[LCS_PROP_Z];
+  for (int64_t i1 = 0; i1 < sp->n; i1++) {
+    int c1[3];
+    decode_cell(sp->ci_hashes[i1], nc, c1);
+    double rho = 0.0;
+    if (c1[0] >= 1 && c1[0] <= nc[0] && c1[1] >= 1 && c1[1] <= nc[1] && c1[2] >= 1 && c1[2] <= nc[2]) {
+      for (int di = -1; di <= 1; di++)
+        for (int dj = -1; dj <= 1; dj++)
+          for (int dk = -1; dk <= 1; dk++) {
+            const int64_t h2 = 1 + (c1[0] + di) + (int64_t)(c1[1] + dj) * (nc[0] + 2) +
+                               (int64_t)(c1[2] + dk) * (nc[0] + 2) * (nc[1] + 2);
+            for (int64_t i2 = sp->ci_starts[h2 - 1]; i2 <= sp->ci_stops[h2 - 1]; i2++) {
+              const double d = norm3(X[i1] - X[i2 - 1], Y[i1] - Y[i2 - 1], Z[i1] - Z[i2 - 1]);
+              if (d < 2 * hh) {
+                /* cubic_spline_kernel (stat.jl:217-227) */
+                const double q = d / hh;
+                double w;
+                if (q < 1) w = factor * (1 - 1.5 * (q * q) + 0.75 * (q * q * q));
+                else if (q < 2) w = factor * 0.25 * ((2 - q) * (2 - q) * (2 - q));
+                else w = 0.0;
+                rho += w;
+              }
+            }
+          }
+    }
+    rho_out[i1] = rho;
+  }
   return LCS_OK;
 }
 int lcs_particles_boundary(lcs_handle* h, int32_t s, int32_t stage) {

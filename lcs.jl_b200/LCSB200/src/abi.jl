@@ -100,3 +100,53 @@ function step!(h, n::Integer)
     logs
 end
 set_state!(h, step, t) = check(h, ccall((:lcs_set_state, LIB), Cint, (Ptr{Cvoid}, Int64, Float64), h, step, t))
+
+# ---- cell index and particle statistics (include/lcs_b200.h) -------------
+const RDF_MAX_BINS = 1024
+const SPECTRUM_MAX_SHELLS = 19
+struct LcsParticleStatConfig
+    grid_ratio::Int32
+    bin_size::Int32
+    search_cell_size::Int32
+    max_wavenumber::Int32
+    nsamples::Int32
+    pad_::Int32
+    contact_tolerance::Float64
+    min_radius::Float64
+end
+struct LcsSummary
+    mean::Float64
+    max::Float64
+    min::Float64
+end
+struct LcsParticleStats
+    x::LcsSummary; y::LcsSummary; z::LcsSummary
+    u::LcsSummary; v::LcsSummary; w::LcsSummary
+    diam::LcsSummary
+    taup::Float64
+    St::Float64
+    gr_contact::Float64
+    npairs_contact::Int64
+    nbins::Int32
+    nshells::Int32
+    edges::NTuple{RDF_MAX_BINS + 1,Float64}
+    gr::NTuple{RDF_MAX_BINS,Float64}
+    npairs::NTuple{RDF_MAX_BINS,Int64}
+    wavenumbers::NTuple{SPECTRUM_MAX_SHELLS,Float64}
+    Enp::NTuple{SPECTRUM_MAX_SHELLS,Float64}
+end
+
+makeindex!(h, s, stage, grid_ratio) =
+    check(h, ccall((:lcs_particles_makeindex, LIB), Cint, (Ptr{Cvoid}, Int32, Int32, Int32), h, s, stage, grid_ratio))
+function particle_stat(h, s, pc::LcsParticleStatConfig, tau_eta::Float64)
+    out = Ref{LcsParticleStats}()
+    check(h, ccall((:lcs_particles_stat, LIB), Cint,
+        (Ptr{Cvoid}, Int32, Ref{LcsParticleStatConfig}, Float64, Ref{LcsParticleStats}), h, s, pc, tau_eta, out))
+    out[]
+end
+function particle_density(h, s, grid_ratio, n)
+    rho = Vector{Float64}(undef, n)
+    check(h, ccall((:lcs_particles_density, LIB), Cint, (Ptr{Cvoid}, Int32, Int32, Ptr{Float64}),
+        h, s, grid_ratio, rho))
+    rho
+end

@@ -154,6 +154,12 @@ LCS_API int lcs_footprint(const lcs_config* cfg, int64_t* bytes);
 /* Interior U,V,W,P in, halos left for the next synchalo (src/flows/inits/init.jl). */
 LCS_API int lcs_upload_flow(lcs_handle* h, const double* U, const double* V, const double* W, const double* P);
 LCS_API int lcs_download_flow(lcs_handle* h, double* U, double* V, double* W, double* P);
+/* The `upsample` init (src/LCSIO/upsample.jl:1-91, flows/config.jl:58-64):
+ * coarse interiors of (nx/2, ny/2, nz/2) cells, as read from a coarse restart,
+ * periodically extended by one cell and trilinearly upsampled 2x into the
+ * interior of U, V, W and P (trilinear_upsample2x!, upsample.jl:47-91).  Dims
+ * must be even; halos are left for the next synchalo. */
+LCS_API int lcs_upload_flow_coarse(lcs_handle* h, const double* U, const double* V, const double* W, const double* P);
 /* Whole field, interior (haloed=0) or haloed (haloed=1) layout. */
 LCS_API int lcs_field_set(lcs_handle* h, int32_t field, const double* data, int32_t haloed);
 LCS_API int lcs_field_get(lcs_handle* h, int32_t field, double* data, int32_t haloed);

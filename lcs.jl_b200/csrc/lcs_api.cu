@@ -173,6 +173,10 @@ int lcs_particles_stat(lcs_handle* h, int32_t s, const lcs_particle_stat_config*
   H(h);
   return h->e->particles_stat(s, pc, tau_eta, out);
 }
+int lcs_upload_flow_coarse(lcs_handle* h, const double* U, const double* V, const double* W, const double* P) {
+  H(h);
+  return h->e->upload_flow_coarse(U, V, W, P);
+}
 int lcs_particles_density(lcs_handle* h, int32_t s, int32_t ratio, double* densities) {
   H(h);
   return h->e->particles_density(s, ratio, densities);

@@ -41,6 +41,7 @@ struct EngineBase {
   virtual int particles_cellindex(int s, int64_t* hashes, int64_t* starts, int64_t* stops) = 0;
   virtual int particles_stat(int s, const lcs_particle_stat_config* pc, double tau_eta, lcs_particle_stats* out) = 0;
   virtual int particles_density(int s, int grid_ratio, double* densities) = 0;
+  virtual int upload_flow_coarse(const double* U, const double* V, const double* W, const double* P) = 0;
   virtual int transfer_stats(int64_t* h2d, int64_t* d2h) = 0;
   virtual int synchalo(int mask, int r, int full) = 0;
   virtual int rhs(int stage) = 0;

@@ -1019,6 +1019,23 @@ class Engine : public EngineBase {
     uploaded_flow = true;
     return LCS_OK;
   }
+  // `load_coarse_flow_fields!` (src/LCSIO/upsample.jl:1-45) after the read:
+  // coarse (n/2)^3 interiors of U, V, W, P, upsampled 2x into the fields
+  int upload_flow_coarse(const double* U, const double* V, const double* W, const double* Pp) override {
+    if (!U || !V || !W || !Pp) return fail(LCS_EINVAL, "null field");
+    if (g.n[0] % 2 || g.n[1] % 2 || g.n[2] % 2) return fail(LCS_EINVAL, "upsampling needs even dims");
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    const int64_t nc = (int64_t)(g.n[0] / 2) * (g.n[1] / 2) * (g.n[2] / 2);
+    const double* src[4] = {U, V, W, Pp};
+    for (int q = 0; q < 4; q++) {
+      LCS_TRY(copy(stage, src[q], (size_t)nc * sizeof(double), cudaMemcpyHostToDevice));
+      LCS_TRY(launch("upsample2x", k_upsample2x<T>, dim3(blocks_for(nc, 256)), dim3(256), 0, (const Ctx*)dctx, g,
+                     q < 3 ? kSetUs : -1, q < 3 ? q : 0, q < 3 ? (T*)nullptr : P, (const double*)stage));
+    }
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    uploaded_flow = true;
+    return LCS_OK;
+  }
   int download_flow(double* U, double* V, double* W, double* Pp) override {
     if (U) LCS_TRY(download_field(kSetUs, 0, nullptr, U, 0));
     if (V) LCS_TRY(download_field(kSetUs, 1, nullptr, V, 0));

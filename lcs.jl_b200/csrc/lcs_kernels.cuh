@@ -1417,6 +1417,37 @@ __global__ void k_scatter(const Ctx* __restrict__ ctx, Grid g, int set, int comp
   }
 }
 
+// trilinear_upsample2x! (src/LCSIO/upsample.jl:47-91): every coarse cell
+// (i, j, k) of the (n/2)^3 interior writes the 8 fine cells (2i-1..2i, ...),
+// the coarse neighbours at i+1 read through the periodic halo (the reference's
+// FullHalo(1) synchalo!).  Sums left to right as written there, in FP64,
+// rounded once to T.
+template <typename T>
+__global__ void __launch_bounds__(256) k_upsample2x(const Ctx* __restrict__ ctx, Grid g, int set, int comp,
+                                                    T* __restrict__ direct, const double* __restrict__ c) {
+  T* f = direct ? direct : (T*)ctx->vel[set][comp];
+  const int nx = g.n[0] / 2, ny = g.n[1] / 2, nz = g.n[2] / 2;
+  const int64_t total = (int64_t)nx * ny * nz;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx), j = (int)((t / nx) % ny), k = (int)(t / ((int64_t)nx * ny));  // 0-based
+    const int i1 = i + 1 < nx ? i + 1 : 0, j1 = j + 1 < ny ? j + 1 : 0, k1 = k + 1 < nz ? k + 1 : 0;
+    auto C = [&](int a, int b, int d) { return c[a + (int64_t)nx * (b + (int64_t)ny * d)]; };
+    const double c000 = C(i, j, k), c100 = C(i1, j, k), c010 = C(i, j1, k), c001 = C(i, j, k1);
+    const double c110 = C(i1, j1, k), c101 = C(i1, j, k1), c011 = C(i, j1, k1), c111 = C(i1, j1, k1);
+    const int ii = 2 * i + 1, jj = 2 * j + 1, kk = 2 * k + 1;  // 1-based fine index 2i-1
+    f[g.at(ii, jj, kk)] = (T)c000;
+    f[g.at(ii + 1, jj, kk)] = (T)(0.5 * __dadd_rn(c000, c100));
+    f[g.at(ii, jj + 1, kk)] = (T)(0.5 * __dadd_rn(c000, c010));
+    f[g.at(ii, jj, kk + 1)] = (T)(0.5 * __dadd_rn(c000, c001));
+    f[g.at(ii + 1, jj + 1, kk)] = (T)(0.25 * __dadd_rn(__dadd_rn(__dadd_rn(c000, c100), c010), c110));
+    f[g.at(ii + 1, jj, kk + 1)] = (T)(0.25 * __dadd_rn(__dadd_rn(__dadd_rn(c000, c100), c001), c101));
+    f[g.at(ii, jj + 1, kk + 1)] = (T)(0.25 * __dadd_rn(__dadd_rn(__dadd_rn(c000, c010), c001), c011));
+    double s8 = __dadd_rn(__dadd_rn(__dadd_rn(c000, c100), c010), c001);
+    s8 = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(s8, c110), c101), c011), c111);
+    f[g.at(ii + 1, jj + 1, kk + 1)] = (T)(0.125 * s8);
+  }
+}
+
 template <typename T>
 __global__ void k_gather(const Ctx* __restrict__ ctx, Grid g, int set, int comp, const T* __restrict__ direct,
                          double* __restrict__ dst, int haloed) {

@@ -247,6 +247,7 @@ PROTOTYPES = {
     "lcs_particles_stat": (C.c_int, [_P, C.c_int32, C.POINTER(ParticleStatConfig), C.c_double,
                                      C.POINTER(ParticleStats)]),
     "lcs_particles_density": (C.c_int, [_P, C.c_int32, C.c_int32, _D]),
+    "lcs_upload_flow_coarse": (C.c_int, [_P, _D, _D, _D, _D]),
     "lcs_step_begin": (C.c_int, [_P, C.c_int32]),
     "lcs_step_poll": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "lcs_step_finish": (C.c_int, [_P, C.POINTER(Log)]),

@@ -101,6 +101,12 @@ class Engine:
         arrs = [_c64(a).reshape(self.interior_shape) for a in (U, V, W, P)]
         self._check(self.lib.lcs_upload_flow(self.handle, *[_dptr(a) for a in arrs]))
 
+    def upload_flow_coarse(self, U, V, W, P):
+        """The `upsample` init (src/LCSIO/upsample.jl:1-91): coarse (n/2)^3
+        interior arrays [k, j, i], upsampled 2x on the device."""
+        arrs = [_c64(a) for a in (U, V, W, P)]
+        self._check(self.lib.lcs_upload_flow_coarse(self.handle, *[_dptr(a) for a in arrs]))
+
     def download_flow(self):
         out = [np.empty(self.interior_shape) for _ in range(4)]
         self._check(self.lib.lcs_download_flow(self.handle, *[_dptr(a) for a in out]))

@@ -965,6 +965,49 @@ int lcs_upload_flow(lcs_handle* h, const double* U, const double* V, const doubl
   return rc ? LCS_EINVAL : LCS_OK;
 }
 
+/* load_coarse_flow_fields! (src/LCSIO/upsample.jl:1-45): the coarse interior
+ * in a (m+2)^3 array with a periodic one-cell halo (the FullHalo(1) synchalo!
+ * on one rank), then trilinear_upsample2x! (upsample.jl:47-91) into the fine
+ * interior, term by term. */
+int lcs_upload_flow_coarse(lcs_handle* h, const double* U, const double* V, const double* W, const double* P) {
+  if (!h || !U || !V || !W || !P) return LCS_EINVAL;
+  const grid_t* g = &h->g;
+  if (g->n[0] % 2 || g->n[1] % 2 || g->n[2] % 2) return fail(h, LCS_EINVAL, "upsampling needs even dims");
+  const int mx = g->n[0] / 2, my = g->n[1] / 2, mz = g->n[2] / 2;
+  const int sx = mx + 2, sy = my + 2, sz = mz + 2;
+  double* Ac = (double*)malloc((size_t)sx * sy * sz * sizeof(double));
+  const double* src[4] = {U, V, W, P};
+  double* dst[4] = {h->U, h->V, h->W, h->P};
+#define AC(i, j, k) Ac[(i) + (size_t)sx * ((j) + (size_t)sy * (k))] /* logical 0..m+1 */
+  for (int q = 0; q < 4; q++) {
+    for (int k = 0; k <= mz + 1; k++)
+      for (int j = 0; j <= my + 1; j++)
+        for (int i = 0; i <= mx + 1; i++) {
+          const int ii = (i + mx - 1) % mx, jj = (j + my - 1) % my, kk = (k + mz - 1) % mz; /* periodic */
+          AC(i, j, k) = src[q][ii + (size_t)mx * (jj + (size_t)my * kk)];
+        }
+    double* F = dst[q];
+    for (int k = 1; k <= mz; k++)
+      for (int j = 1; j <= my; j++)
+        for (int i = 1; i <= mx; i++) {
+          const int a = 2 * i - 1, b = 2 * j - 1, c = 2 * k - 1;
+          F[IX(g, a, b, c)] = AC(i, j, k);
+          F[IX(g, a + 1, b, c)] = (1.0 / 2) * (AC(i, j, k) + AC(i + 1, j, k));
+          F[IX(g, a, b + 1, c)] = (1.0 / 2) * (AC(i, j, k) + AC(i, j + 1, k));
+          F[IX(g, a, b, c + 1)] = (1.0 / 2) * (AC(i, j, k) + AC(i, j, k + 1));
+          F[IX(g, a + 1, b + 1, c)] = (1.0 / 4) * (AC(i, j, k) + AC(i + 1, j, k) + AC(i, j + 1, k) + AC(i + 1, j + 1, k));
+          F[IX(g, a + 1, b, c + 1)] = (1.0 / 4) * (AC(i, j, k) + AC(i + 1, j, k) + AC(i, j, k + 1) + AC(i + 1, j, k + 1));
+          F[IX(g, a, b + 1, c + 1)] = (1.0 / 4) * (AC(i, j, k) + AC(i, j + 1, k) + AC(i, j, k + 1) + AC(i, j + 1, k + 1));
+          F[IX(g, a + 1, b + 1, c + 1)] =
+              (1.0 / 8) * (AC(i, j, k) + AC(i + 1, j, k) + AC(i, j + 1, k) + AC(i, j, k + 1) + AC(i + 1, j + 1, k) +
+                           AC(i + 1, j, k + 1) + AC(i, j + 1, k + 1) + AC(i + 1, j + 1, k + 1));
+        }
+  }
+#undef AC
+  free(Ac);
+  return LCS_OK;
+}
+
 int lcs_download_flow(lcs_handle* h, double* U, double* V, double* W, double* P) {
   int rc = 0;
   if (U) rc |= lcs_field_get(h, LCS_FIELD_U, U, 0);

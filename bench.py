@@ -738,6 +738,9 @@ def main():
         return run_reference(args)
     if args.report == "precision":
         return run_precision_report(args)
+    if args.workload in ("batch64", "serve"):
+        # one hardware work queue per member stream (read at context creation)
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     if args.workload == "batch64":
         return run_batch(args)
     if args.workload == "serve":

@@ -329,7 +329,10 @@ LCS_API int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, doubl
  * so the members' kernels overlap on the GPU.  Each member computes exactly
  * what it computes alone.  Members are ordinary handles (lcs_batch_member) for
  * uploads, downloads and single-member calls between batch steps; the batch
- * owns and destroys them.  logs is member-major: logs[i * nsteps + q]. */
+ * owns and destroys them.  logs is member-major: logs[i * nsteps + q].
+ * lcs_batch_create and lcs_server_create set CUDA_DEVICE_MAX_CONNECTIONS=32
+ * (unless already set) so that up to 32 member streams get their own hardware
+ * work queue; it takes effect only if the process has no CUDA context yet. */
 typedef struct lcs_batch lcs_batch;
 LCS_API int lcs_batch_create(const lcs_config* members, int32_t m, lcs_batch** out);
 LCS_API int lcs_batch_size(const lcs_batch* b, int32_t* m);

@@ -154,6 +154,14 @@ int autotune(lcs_batch* b) {
   return LCS_OK;
 }
 
+// Members and served runs step on their own streams.  CUDA maps streams onto
+// CUDA_DEVICE_MAX_CONNECTIONS hardware work queues (8 unless set); streams
+// beyond that share queues and serialise behind each other's launches.  The
+// variable is read when the process creates its CUDA context, so this widens
+// the queues to the maximum (32) only when no context exists yet and the user
+// has not chosen a value.
+void widen_work_queues() { setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0); }
+
 }  // namespace
 
 extern "C" {
@@ -164,6 +172,7 @@ int lcs_batch_create(const lcs_config* members, int32_t m, lcs_batch** out) {
   if (!out) return serve_fail(LCS_EINVAL, "null output");
   *out = nullptr;
   if (!members || m < 1) return serve_fail(LCS_EINVAL, "a batch needs at least one member config");
+  widen_work_queues();
   std::unique_ptr<lcs_batch> b(new lcs_batch);
   for (int32_t i = 0; i < m; i++) {
     lcs_config c = members[i];
@@ -502,6 +511,7 @@ int lcs_server_create(const lcs_server_config* c, lcs_server** out) {
   if (c->steps_per_slice < 1 || c->steps_per_slice > LCS_MAX_ASYNC_STEPS)
     return serve_fail(LCS_EINVAL, "steps_per_slice out of range");
   if (c->hbm_budget_bytes <= 0) return serve_fail(LCS_EINVAL, "hbm_budget_bytes must be positive");
+  widen_work_queues();
   std::unique_ptr<lcs_server> s(new lcs_server);
   s->cfg = *c;
   s->th = std::thread([p = s.get()] { p->run(); });

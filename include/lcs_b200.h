@@ -335,6 +335,20 @@ LCS_API int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, doubl
  * work queue; it takes effect only if the process has no CUDA context yet. */
 typedef struct lcs_batch lcs_batch;
 LCS_API int lcs_batch_create(const lcs_config* members, int32_t m, lcs_batch** out);
+/* A group: 2..64 handles of one shape (dims, halo, HSMAC settings, precision)
+ * and one set of launch shapes (lcs_set_tuning) whose steps run as one CUDA
+ * graph.  Each member's own kernels run member after member; each couple's
+ * HSMAC loop is one device-side loop for the whole group whose sweep, halo and
+ * face kernels are launched once for all members (a member computes exactly
+ * what it computes alone with the same launch shapes).  lcs_group_step_begin
+ * enqueues nsteps steps of every member; lcs_step_poll / lcs_step_finish on
+ * each member then complete them as for lcs_step_begin.  The group does not
+ * own its members; destroy it before them.  lcs_batch_create groups members
+ * this way by itself. */
+typedef struct lcs_group lcs_group;
+LCS_API int lcs_group_create(lcs_handle* const* members, int32_t m, lcs_group** out);
+LCS_API int lcs_group_step_begin(lcs_group* group, int32_t nsteps);
+LCS_API void lcs_group_destroy(lcs_group* group);
 LCS_API int lcs_batch_size(const lcs_batch* b, int32_t* m);
 LCS_API int lcs_batch_member(lcs_batch* b, int32_t i, lcs_handle** h);
 LCS_API int lcs_batch_step(lcs_batch* b, int32_t nsteps, lcs_log* logs);

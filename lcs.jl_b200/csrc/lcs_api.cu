@@ -2,6 +2,7 @@
 // Each call validates its arguments, forwards to the handle's engine, and
 // turns every failure into a status code plus a message (no exceptions or
 // aborts cross the ABI).
+#include <vector>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -172,6 +173,35 @@ int lcs_particles_stat(lcs_handle* h, int32_t s, const lcs_particle_stat_config*
                        lcs_particle_stats* out) {
   H(h);
   return h->e->particles_stat(s, pc, tau_eta, out);
+}
+struct lcs_group {
+  lcs::GroupBase* g;
+};
+int lcs_group_create(lcs_handle* const* members, int32_t m, lcs_group** out) {
+  if (!out) return set_global_error(LCS_EINVAL, "null output");
+  *out = nullptr;
+  if (!members || m < 2) return set_global_error(LCS_EINVAL, "a group needs at least two handles");
+  std::vector<lcs::EngineBase*> es;
+  for (int32_t q = 0; q < m; q++) {
+    if (!members[q]) return set_global_error(LCS_EINVAL, "null group member");
+    es.push_back(members[q]->e);
+  }
+  lcs::GroupBase* g = nullptr;
+  const int rc = es[0]->group_create(es.data(), m, &g);
+  if (rc != LCS_OK) return set_global_error(rc, es[0]->err.c_str());
+  *out = new lcs_group{g};
+  return LCS_OK;
+}
+int lcs_group_step_begin(lcs_group* gr, int32_t nsteps) {
+  if (!gr) return set_global_error(LCS_EINVAL, "null group");
+  const int rc = gr->g->step_begin(nsteps);
+  if (rc != LCS_OK) return set_global_error(rc, gr->g->err.c_str());
+  return LCS_OK;
+}
+void lcs_group_destroy(lcs_group* gr) {
+  if (!gr) return;
+  delete gr->g;
+  delete gr;
 }
 int lcs_upload_flow_coarse(lcs_handle* h, const double* U, const double* V, const double* W, const double* P) {
   H(h);

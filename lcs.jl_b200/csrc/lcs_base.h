@@ -10,6 +10,23 @@
 
 namespace lcs {
 
+// A batch group (lcs_group_*): handles of one shape and launch shapes whose
+// steps run as one CUDA graph with group-wide HSMAC launches.
+struct GroupBase {
+  std::string err;
+  virtual ~GroupBase() {}
+  virtual int step_begin(int nsteps) = 0;
+  int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+  }
+};
+
 struct EngineBase {
   std::string err;
   virtual ~EngineBase() {}
@@ -61,6 +78,7 @@ struct EngineBase {
   virtual int profile_entry(int i, char* name, int cap, double* ms, int64_t* launches) = 0;
   virtual int launch_count(int64_t* n) = 0;
   virtual int synchronize() = 0;
+  virtual int group_create(EngineBase* const* members, int m, GroupBase** out) = 0;
   int fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;

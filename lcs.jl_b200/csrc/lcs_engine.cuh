@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "../../include/lcs_b200.h"
@@ -174,6 +175,12 @@ class Engine : public EngineBase {
   // first index): the permutation writes the spare block and the two swap.
   uint64_t* sp_alloc[LCS_MAX_SPECIES] = {};  // owned (cudaMalloc)
   uint64_t* sp_spare[LCS_MAX_SPECIES] = {};  // the block not in use (sp_alloc or the one in the pool)
+  // Batch group (EngineGroup): while the leader captures the group's HSMAC
+  // loop, grp lists the members and the HSMAC launches cover all of them.
+  const std::vector<Engine<T>*>* grp = nullptr;
+  int tuning_gen = 0;            // bumped by set_tuning (a group's graph is rebuilt)
+  GroupPtrs<T> grp_ptrs{};       // per member Ctx, P, partials (set by the group)
+  int face_group_per_sm = 0;     // co-resident blocks per SM of k_hsmac_faces_group
   // scratch of the particle statistics (grown on demand)
   char* pbuf = nullptr;
   size_t pbuf_bytes = 0;
@@ -404,6 +411,10 @@ class Engine : public EngineBase {
                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (rp != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (row-warp P) failed: %d", (int)rp);
     LCS_CUDA(cudaFuncSetAttribute(rw_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
+    const void* rw_group_fn = rw_variant == 1   ? (const void*)k_hsmac_rw_group<T, 8, 3>
+                              : rw_variant == 2 ? (const void*)k_hsmac_rw_group<T, 5, 3>
+                                                : (const void*)k_hsmac_rw_group<T, 13, 3>;
+    LCS_CUDA(cudaFuncSetAttribute(rw_group_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
     LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rw_ctas_per_sm, rw_fn, rw_threads, rw_smem));
     if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the row-warp sweep does not fit on an SM");
     return LCS_OK;
@@ -426,6 +437,7 @@ class Engine : public EngineBase {
     const char* f = std::getenv("LCS_B200_FACES");
     const bool sequential = f && std::string(f) == "phases";
     face_grid = (coop && per_sm > 0 && !sequential) ? std::min(per_sm, 2) * num_sms : 0;
+    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&face_group_per_sm, k_hsmac_faces_group<T>, 256, 0));
     return LCS_OK;
   }
 
@@ -556,6 +568,7 @@ class Engine : public EngineBase {
 
   // ------------------------------------------------------------ primitives
   int fill(int set, bool withP, int r, int full) {
+    if (grp && withP) return fail(LCS_EINVAL, "group fills carry no P");
     FillArgs fa;
     memset(&fa, 0, sizeof fa);
     fa.nf = 0;
@@ -564,6 +577,9 @@ class Engine : public EngineBase {
     if (withP) { fa.set[fa.nf] = -1; fa.comp[fa.nf] = 0; fa.ptr[fa.nf] = P; fa.nf++; }
     const int64_t total = fill_count(g, r, full);
     if (total >= INT32_MAX) return fail(LCS_EINVAL, "halo too large for 32-bit fill indices");
+    if (grp)
+      return launch("synchalo", k_fill_halo_group<T>, dim3(blocks_for(total, 256, 148 * 32), (unsigned)grp->size()),
+                    dim3(256), 0, grp_ptrs, g, fa, r, full, total);
     return launch("synchalo", k_fill_halo<T>, dim3(blocks_for(total, 256, 148 * 32)), dim3(256), 0, (const Ctx*)dctx, g, fa, r,
                   full, total);
   }
@@ -601,6 +617,7 @@ class Engine : public EngineBase {
     return f;
   }
   int fused(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks = nullptr) {
+    if (grp && !use_rw) return fail(LCS_EINVAL, "group sweeps need the row-warp sweep");
     if (use_tma) return fused_tma(set, D, out, fill_r, part, finalize, group_end, nblocks);
     const FusedGeom f = fused_geom(out);
     const int64_t nb = (int64_t)f.gx * f.gy * f.gz;
@@ -672,6 +689,7 @@ class Engine : public EngineBase {
     const int nitems = sc.nitems;
     if (nitems > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
     if (nblocks) *nblocks = nitems;
+    if (grp) return fused_rw_group(set, D, out, gb, xo, gx, gy, sc, finalize, group_end);
     const dim3 grid(nitems), block(rw_threads);
     switch (rw_variant) {
       case 1: return launch("hsmac_rw", k_hsmac_rw<T, 8, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P, D,
@@ -681,6 +699,34 @@ class Engine : public EngineBase {
       default: return launch("hsmac_rw", k_hsmac_rw<T, 13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P,
                              D, out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
     }
+  }
+  // the same sweep for every member of the group, kGroupMax members a launch
+  int fused_rw_group(int set, Box D, Box out, Box gb, int xo, int gx, int gy, RwSched sc, int finalize, int group_end) {
+    const int M = (int)grp->size();
+    for (int m0 = 0; m0 < M; m0 += kGroupMax) {
+      const int mc = std::min(kGroupMax, M - m0);
+      GroupRwArgs<T> ga;
+      memset(&ga, 0, sizeof ga);
+      for (int q = 0; q < mc; q++) {
+        Engine<T>* e = (*grp)[m0 + q];
+        ga.tm[q] = e->tmaps_rw;
+        ga.ctx[q] = e->dctx;
+        ga.P[q] = e->P;
+        ga.partials[q] = e->partials;
+      }
+      const dim3 grid(sc.nitems, mc), block(rw_threads);
+      int rc2;
+      switch (rw_variant) {
+        case 1: rc2 = launch("hsmac_rw", k_hsmac_rw_group<T, 8, 3>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
+                             gx, gy, sc, hc, finalize, group_end); break;
+        case 2: rc2 = launch("hsmac_rw", k_hsmac_rw_group<T, 5, 3>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
+                             gx, gy, sc, hc, finalize, group_end); break;
+        default: rc2 = launch("hsmac_rw", k_hsmac_rw_group<T, 13, 3>, grid, block, rw_smem, ga, g, set, D, out, gb,
+                              xo, gx, gy, sc, hc, finalize, group_end);
+      }
+      LCS_TRY(rc2);
+    }
+    return LCS_OK;
   }
   int fused_tma(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
     if (use_rw) return fused_rw(set, D, out, fill_r, part, finalize, group_end, nblocks);
@@ -709,6 +755,7 @@ class Engine : public EngineBase {
 
   // in-place colour phases over a box (both colours), partial sums appended
   int phases(int set, Box b, double* part, int* used) {
+    if (grp) return fail(LCS_EINVAL, "group sweeps need the cooperative face kernel");
     if (b.lo[0] > b.hi[0] || b.lo[1] > b.hi[1] || b.lo[2] > b.hi[2]) return LCS_OK;
     if (cfg.coloring == LCS_COLORING_RED_BLACK_BLOCK) {
       const int bs = cfg.coloring_block;
@@ -740,6 +787,7 @@ class Engine : public EngineBase {
     out[5].lo[0] = c.hi[0] + 1; out[5].lo[1] = c.lo[1]; out[5].hi[1] = c.hi[1]; out[5].lo[2] = c.lo[2]; out[5].hi[2] = c.hi[2];
   }
   int finalize_sweep(int n, int group_end) {
+    if (grp) return fail(LCS_EINVAL, "group sweeps finalize inside the sweep kernels");
     return launch("hsmac_finalize", k_hsmac_finalize, dim3(1), dim3(256), 0, dctx, (const double*)partials, n, hc,
                   group_end);
   }
@@ -771,6 +819,24 @@ class Engine : public EngineBase {
         used + fblocks <= plan.partials_cap && 2 * slab_cells < INT32_MAX) {
       FaceSet fs;
       for (int q = 0; q < 6; q++) fs.f[q] = f[q];
+      if (grp) {  // members in co-resident chunks; each member's blocks meet at its own barrier
+        const int M = (int)grp->size();
+        const int per = std::max(1, std::min(kGroupPtrMax, face_group_per_sm * num_sms / fblocks));
+        if (face_group_per_sm * num_sms < fblocks) return fail(LCS_EINVAL, "face grid too large for a group");
+        for (int m0 = 0; m0 < M; m0 += per) {
+          const int mc = std::min(per, M - m0);
+          GroupPtrs<T> gp;
+          memset(&gp, 0, sizeof gp);
+          for (int q = 0; q < mc; q++) {
+            gp.ctx[q] = grp_ptrs.ctx[m0 + q];
+            gp.P[q] = grp_ptrs.P[m0 + q];
+            gp.partials[q] = grp_ptrs.partials[m0 + q];
+          }
+          LCS_TRY(launch_coop("hsmac_faces", k_hsmac_faces_group<T>, dim3(fblocks, mc), dim3(256), gp, g, set, fs,
+                              hc, used, group_end));
+        }
+        return LCS_OK;
+      }
       return launch_coop("hsmac_faces", k_hsmac_faces<T>, dim3(fblocks), dim3(256), dctx, g, set, P, fs, hc,
                          partials, used, group_end);
     }
@@ -1217,6 +1283,7 @@ class Engine : public EngineBase {
     }
     zchunk_force = zchunk;
     sm_share = share;
+    tuning_gen++;
     drop_graphs();
     return LCS_OK;
   }
@@ -1246,6 +1313,11 @@ class Engine : public EngineBase {
       LCS_CUDA(cudaGraphLaunch(step_exec, stream));
       launches += graph_launches_per_step;
     }
+    return async_tail(nsteps);
+  }
+  // After nsteps enqueued steps: the context and the steps' logs back into
+  // pinned memory, and the event step_poll/step_finish wait for.
+  int async_tail(int nsteps) {
     LCS_TRY(copy(hctx, dctx, sizeof(Ctx), cudaMemcpyDeviceToHost));
     const int64_t cap = plan.logs_cap, i0 = host_step % cap;  // ring index of step host_step + 1
     const int64_t n1 = std::min<int64_t>(nsteps, cap - i0);
@@ -1255,6 +1327,16 @@ class Engine : public EngineBase {
     async_pending = nsteps;
     return LCS_OK;
   }
+  // checks of a handle before steps are enqueued for it (alone or in a group)
+  int async_ready(int nsteps) {
+    LCS_TRY(check_flow());
+    if (async_pending) return fail(LCS_ESTATE, "steps are already in flight on this handle");
+    if (nsteps < 1 || nsteps > plan.logs_cap) return fail(LCS_EINVAL, "nsteps must be in 1..%lld", (long long)plan.logs_cap);
+    if (prof) return fail(LCS_ESTATE, "asynchronous steps do not run with profiling on");
+    if (!host_step_known) LCS_TRY(read_ctx());
+    return LCS_OK;
+  }
+  int group_create(EngineBase* const* members, int m, GroupBase** out) override;
   int step_poll(int* done) override {
     if (!done) return fail(LCS_EINVAL, "null output");
     if (!async_pending) return fail(LCS_ESTATE, "no steps in flight on this handle");
@@ -1786,5 +1868,205 @@ class Engine : public EngineBase {
     return LCS_OK;
   }
 };
+
+// ---------------------------------------------------------------- batch group
+// Handles of one shape (dims, halo, HSMAC settings, precision) and one set of
+// launch shapes (tile rows, z chunk, GPU share) step as one CUDA graph on the
+// first member's stream.  Each member's own kernels (time step, halo fill,
+// particles, rhs/update, forcing, logs) are captured member after member;
+// the HSMAC loop of each couple is one conditional WHILE node for the whole
+// group whose body launches every sweep kernel once for all members
+// (blockIdx.y = member): a member's blocks do exactly what its own launch
+// does, so each member computes what it computes alone with the same launch
+// shapes, and a member whose loop has ended returns at once.
+template <typename T>
+struct EngineGroup : GroupBase {
+  std::vector<Engine<T>*> mem;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<int64_t> per_step;
+  std::vector<int> gens;
+  cudaEvent_t ready = nullptr;
+  ~EngineGroup() override {
+    if (mem.size()) cudaStreamSynchronize(mem[0]->stream);
+    drop();
+    if (ready) cudaEventDestroy(ready);
+  }
+  void drop() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  int member_fail(Engine<T>* m, int rc) { return fail(rc, "%s", m->err.c_str()); }
+#define LCS_GTRY(m, expr)                              \
+  do {                                                 \
+    int rc_ = (expr);                                  \
+    if (rc_ != LCS_OK) return member_fail((m), rc_);   \
+  } while (0)
+
+  int couple_nodes(int stage) {
+    Engine<T>* L = mem[0];
+    const int set = stage == 1 ? kSetUs2 : kSetUs;
+    for (auto* m : mem)
+      LCS_GTRY(m, m->launch("couple_reset", k_couple_reset, dim3(1), dim3(1), 0, m->dctx, m->cfg.itrmax));
+    cudaStream_t s = L->stream;
+    cudaStreamCaptureStatus st;
+    cudaGraph_t gr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    LCS_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &gr, &deps, &ndeps));
+    if (st != cudaStreamCaptureStatusActive) return fail(LCS_ESTATE, "group couple outside a capture");
+    cudaGraphConditionalHandle handle;
+    LCS_CUDA(cudaGraphConditionalHandleCreate(&handle, gr, L->cfg.itrmax > 0 ? 1u : 0u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    LCS_CUDA(cudaGraphAddNode(&node, gr, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaStream_t side;
+    LCS_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    cudaError_t eb = cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    int rc2 = eb == cudaSuccess ? LCS_OK : fail(LCS_ECUDA, "capture of the group loop: %s", cudaGetErrorString(eb));
+    if (rc2 == LCS_OK) {
+      L->stream = side;
+      L->grp = &mem;
+      rc2 = L->couple_group(set);
+      if (rc2 == LCS_OK)
+        rc2 = L->launch("couple_continue", k_group_continue<T>, dim3(1), dim3(1), 0, L->grp_ptrs, (int)mem.size(),
+                        handle);
+      L->grp = nullptr;
+      L->stream = s;
+      if (rc2 != LCS_OK) rc2 = member_fail(L, rc2);
+      cudaGraph_t body_out;
+      cudaError_t e = cudaStreamEndCapture(side, &body_out);
+      if (rc2 == LCS_OK && e != cudaSuccess) rc2 = fail(LCS_ECUDA, "capture of the group loop: %s", cudaGetErrorString(e));
+    }
+    cudaStreamDestroy(side);
+    if (rc2 != LCS_OK) return rc2;
+    LCS_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    for (auto* m : mem) LCS_GTRY(m, m->launch("couple_log", k_couple_log, dim3(1), dim3(1), 0, m->dctx, stage));
+    return LCS_OK;
+  }
+  int capture_step() {
+    for (auto* m : mem) LCS_GTRY(m, m->timestep_kernels(0, nullptr));
+    for (auto* m : mem) LCS_GTRY(m, m->launch("step_begin", k_step_begin, dim3(1), dim3(1), 0, m->dctx));
+    for (int stage = 1; stage <= 2; stage++) {
+      const int set = stage == 1 ? kSetUs : kSetUs2;
+      for (auto* m : mem) {
+        LCS_GTRY(m, m->set_stage_dt(stage));
+        LCS_GTRY(m, m->fill(set, true, m->g.h, 1));
+        LCS_GTRY(m, m->particles_stage(stage, 7, 1, 0.0));
+        LCS_GTRY(m, m->rhs_kernel(set, stage == 1 ? kSetUs2 : kSetUs, 1, 1, 0.0));
+        if (stage == 2) LCS_GTRY(m, m->forcing_stage());
+      }
+      LCS_TRY(couple_nodes(stage));
+    }
+    for (auto* m : mem)
+      LCS_GTRY(m, m->launch("step_end", k_step_end, dim3(1), dim3(1), 0, m->dctx, m->dlogs, (int)m->plan.logs_cap));
+    return LCS_OK;
+  }
+#undef LCS_GTRY
+  int build() {
+    Engine<T>* L = mem[0];
+    cudaStream_t s = L->stream;
+    std::vector<cudaStream_t> saved(mem.size());
+    LCS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    for (size_t q = 0; q < mem.size(); q++) {
+      saved[q] = mem[q]->stream;
+      mem[q]->stream = s;
+      mem[q]->capturing = true;
+      per_step[q] = mem[q]->launches;
+    }
+    int rc2 = capture_step();
+    for (size_t q = 0; q < mem.size(); q++) {
+      mem[q]->stream = saved[q];
+      mem[q]->capturing = false;
+      per_step[q] = mem[q]->launches - per_step[q];
+      mem[q]->launches -= per_step[q];
+    }
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &gr);
+    if (rc2 != LCS_OK) {
+      if (gr) cudaGraphDestroy(gr);
+      return rc2;
+    }
+    if (e != cudaSuccess) return fail(LCS_ECUDA, "group graph capture: %s", cudaGetErrorString(e));
+    graph = gr;
+    LCS_CUDA(cudaGraphInstantiate(&exec, gr, 0));
+    for (size_t q = 0; q < mem.size(); q++) gens[q] = mem[q]->tuning_gen;
+    return LCS_OK;
+  }
+  int step_begin(int nsteps) override {
+    for (auto* m : mem)
+      if (int rc2 = m->async_ready(nsteps)) return member_fail(m, rc2);
+    for (auto* m : mem)  // a member retuned alone since the group was made: its tiles no longer match
+      if (m->rw_variant != mem[0]->rw_variant || m->zchunk_force != mem[0]->zchunk_force ||
+          m->sm_share != mem[0]->sm_share)
+        return fail(LCS_EINVAL, "group members differ in launch shapes");
+    for (size_t q = 0; q < mem.size(); q++)
+      if (gens[q] != mem[q]->tuning_gen) drop();
+    if (!exec) LCS_TRY(build());
+    Engine<T>* L = mem[0];
+    cudaStream_t s = L->stream;
+    for (size_t q = 1; q < mem.size(); q++) {  // the members' own earlier work first
+      LCS_CUDA(cudaEventRecord(ready, mem[q]->stream));
+      LCS_CUDA(cudaStreamWaitEvent(s, ready, 0));
+    }
+    for (int q = 0; q < nsteps; q++) LCS_CUDA(cudaGraphLaunch(exec, s));
+    for (size_t q = 0; q < mem.size(); q++) {
+      Engine<T>* m = mem[q];
+      m->launches += per_step[q] * nsteps;
+      cudaStream_t own = m->stream;
+      m->stream = s;
+      const int rc2 = m->async_tail(nsteps);
+      m->stream = own;
+      if (rc2 != LCS_OK) return member_fail(m, rc2);
+    }
+    return LCS_OK;
+  }
+};
+
+template <typename T>
+int Engine<T>::group_create(EngineBase* const* members, int m, GroupBase** out) {
+  *out = nullptr;
+  if (m < 2 || m > kGroupPtrMax) return fail(LCS_EINVAL, "a group has 2..%d members", kGroupPtrMax);
+  std::unique_ptr<EngineGroup<T>> gp(new EngineGroup<T>);
+  for (int q = 0; q < m; q++) {
+    Engine<T>* e = dynamic_cast<Engine<T>*>(members[q]);
+    if (!e) return fail(LCS_EINVAL, "group member %d has another precision", q);
+    for (auto* o : gp->mem)
+      if (o == e) return fail(LCS_EINVAL, "group member %d appears twice", q);
+    gp->mem.push_back(e);
+  }
+  Engine<T>* L = gp->mem[0];
+  if (L != this) return fail(LCS_EINVAL, "the first member creates the group");
+  for (auto* e : gp->mem) {
+    const lcs_config &a = L->cfg, &b = e->cfg;
+    const bool same = a.dims[0] == b.dims[0] && a.dims[1] == b.dims[1] && a.dims[2] == b.dims[2] &&
+                      a.halo_size == b.halo_size && a.device == b.device && a.time_blocking == b.time_blocking &&
+                      a.overlap == b.overlap && a.coloring == b.coloring && a.coloring_block == b.coloring_block &&
+                      a.omega == b.omega && a.epsp == b.epsp && a.itrmin == b.itrmin && a.itrmax == b.itrmax;
+    if (!same) return fail(LCS_EINVAL, "group members differ in shape or HSMAC settings");
+    if (!e->use_rw) return fail(LCS_EINVAL, "group members need the row-warp sweep");
+    if (e->rw_variant != L->rw_variant || e->zchunk_force != L->zchunk_force || e->sm_share != L->sm_share)
+      return fail(LCS_EINVAL, "group members differ in launch shapes");
+    if (e->async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on a member");
+    if (e->face_grid <= 0) return fail(LCS_EINVAL, "group members need the cooperative face kernel");
+  }
+  memset(&L->grp_ptrs, 0, sizeof L->grp_ptrs);
+  for (int q = 0; q < m; q++) {
+    L->grp_ptrs.ctx[q] = gp->mem[q]->dctx;
+    L->grp_ptrs.P[q] = gp->mem[q]->P;
+    L->grp_ptrs.partials[q] = gp->mem[q]->partials;
+  }
+  gp->per_step.assign(m, 0);
+  gp->gens.assign(m, -1);
+  LCS_CUDA(cudaEventCreateWithFlags(&gp->ready, cudaEventDisableTiming));
+  *out = gp.release();
+  return LCS_OK;
+}
 
 }  // namespace lcs

@@ -147,11 +147,14 @@ struct RwBits {
 // in FP64, x0 = 3 mod 4 in FP32): the TMA boxes start there and every pair
 // (x0-2+2l, x0-1+2l) is aligned to its own size.  Work items are
 // (z chunk, tile column), chunk major, as in k_hsmac_tma.
+// The sweep of one handle as block `bid` of `nb` (k_hsmac_rw: the launch's
+// own grid; k_hsmac_rw_group: one handle per blockIdx.y).
 template <typename T, int TY, int NS>
-__global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::MINB)
-    k_hsmac_rw(Ctx* __restrict__ ctx, Grid g, int set, const __grid_constant__ TensorMaps tm,
-               T* __restrict__ P, Box D, Box out, Box gb, int x_origin, int gx, int gy, RwSched sc,
-               HsmacCoef cf, double* __restrict__ partials, int finalize, int group_end) {
+__device__ __forceinline__ void hsmac_rw_body(Ctx* __restrict__ ctx, const Grid& g, int set, const TensorMaps& tm,
+                                              T* __restrict__ P, const Box& D, const Box& out, const Box& gb,
+                                              int x_origin, int gx, int gy, const RwSched& sc, const HsmacCoef& cf,
+                                              double* __restrict__ partials, int finalize, int group_end,
+                                              const unsigned int bid, const unsigned int nb) {
   using L = RwLayout<T, TY, NS>;
   using T2 = pair_t<T>;
   constexpr int NT = L::NT, VT = L::VT, DP = L::DP, W = RW_W;
@@ -185,7 +188,7 @@ __global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::
     __syncthreads();
     int loads = 0;  // plane loads issued by this CTA: slot = index % NS, parity = (index / NS) & 1
     bool ok = true;
-    for (int item = blockIdx.x; item < sc.nitems && ok; item += gridDim.x) {
+    for (int item = (int)bid; item < sc.nitems && ok; item += (int)nb) {
       int col, kb, ke;
       rw_item(sc, gb.lo[2], gb.hi[2], item, &col, &kb, &ke);
       if (kb > ke) continue;  // an empty sub-range (uniform in the CTA)
@@ -466,8 +469,6 @@ __global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::
   }
   // residual partial of this CTA; the last CTA finalizes the sweep and swaps
   const double bs = block_sum<NT>(racc, red);
-  const unsigned int nb = gridDim.x;
-  const unsigned int bid = blockIdx.x;
   if (tid == 0) partials[bid] = bs;
   if (last_block(&ctx->ticket, nb, last_flag)) {
     if (skip || ctx->wait_error) {
@@ -495,6 +496,37 @@ __global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::
       }
     }
   }
+}
+
+template <typename T, int TY, int NS>
+__global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::MINB)
+    k_hsmac_rw(Ctx* __restrict__ ctx, Grid g, int set, const __grid_constant__ TensorMaps tm,
+               T* __restrict__ P, Box D, Box out, Box gb, int x_origin, int gx, int gy, RwSched sc,
+               HsmacCoef cf, double* __restrict__ partials, int finalize, int group_end) {
+  hsmac_rw_body<T, TY, NS>(ctx, g, set, tm, P, D, out, gb, x_origin, gx, gy, sc, cf, partials, finalize, group_end,
+                           blockIdx.x, gridDim.x);
+}
+
+// Handles of the same shape and launch shapes swept in one launch (a batch
+// group): blockIdx.y picks the handle; each handle's blocks do exactly what
+// its own k_hsmac_rw launch does, so its fields and residual are those of the
+// handle alone.  The tensor maps travel as kernel parameters (__grid_constant__)
+// like the single-handle launch.
+constexpr int kGroupMax = 24;
+template <typename T>
+struct GroupRwArgs {
+  TensorMaps tm[kGroupMax];
+  Ctx* ctx[kGroupMax];
+  T* P[kGroupMax];
+  double* partials[kGroupMax];
+};
+template <typename T, int TY, int NS>
+__global__ void __launch_bounds__(RwLayout<T, TY, NS>::NT, RwLayout<T, TY, NS>::MINB)
+    k_hsmac_rw_group(const __grid_constant__ GroupRwArgs<T> ga, Grid g, int set, Box D, Box out, Box gb,
+                     int x_origin, int gx, int gy, RwSched sc, HsmacCoef cf, int finalize, int group_end) {
+  const int m = blockIdx.y;
+  hsmac_rw_body<T, TY, NS>(ga.ctx[m], g, set, ga.tm[m], ga.P[m], D, out, gb, x_origin, gx, gy, sc, cf,
+                           ga.partials[m], finalize, group_end, blockIdx.x, gridDim.x);
 }
 }  // namespace
 }  // namespace lcs

@@ -83,8 +83,8 @@ struct FillArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_fill_halo(const Ctx* __restrict__ ctx, Grid g, FillArgs fa, int r, int full,
-                                                   int64_t total) {
+__device__ __forceinline__ void fill_halo_body(const Ctx* __restrict__ ctx, const Grid& g, const FillArgs& fa, int r,
+                                               int full, int64_t total) {
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
   const int wx = full ? nx + 2 * r : nx, wy = full ? ny + 2 * r : ny;
   const int bx = full ? 1 - r : 1, by = full ? 1 - r : 1;
@@ -122,6 +122,11 @@ __global__ void __launch_bounds__(256) k_fill_halo(const Ctx* __restrict__ ctx, 
     for (int q = 0; q < 4; q++)
       if (q < fa.nf) f[q][dst] = f[q][src];
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_fill_halo(const Ctx* __restrict__ ctx, Grid g, FillArgs fa, int r, int full,
+                                                   int64_t total) {
+  fill_halo_body<T>(ctx, g, fa, r, full, total);
 }
 
 inline int64_t fill_count(const Grid& g, int r, int full) {
@@ -447,10 +452,14 @@ __device__ __forceinline__ bool face_locate(const Grid& g, const Box& b, int t, 
 // them, the same in-place result as the twelve sequential launches.  Then
 // the block partials join the core sweep's partials[0, part0), and the last
 // block runs the exit test (k_hsmac_finalize's work).
+// Block `bid` of `nb` of one handle's face phases (k_hsmac_faces: the launch's
+// grid; k_hsmac_faces_group: one handle per blockIdx.y, each handle's blocks
+// meeting at the handle's own grid barrier).
 template <typename T>
-__global__ void __launch_bounds__(256) k_hsmac_faces(Ctx* __restrict__ ctx, Grid g, int set, T* __restrict__ P,
-                                                     FaceSet fs, HsmacCoef cf, double* __restrict__ partials,
-                                                     int part0, int group_end) {
+__device__ __forceinline__ void hsmac_faces_body(Ctx* __restrict__ ctx, const Grid& g, int set, T* __restrict__ P,
+                                                 const FaceSet& fs, const HsmacCoef& cf,
+                                                 double* __restrict__ partials, int part0, int group_end,
+                                                 const unsigned int bid, const unsigned int nb) {
   __shared__ double sh[8];
   __shared__ int flag;
   if (ctx->cs.done) return;  // written before this launch: the same in every block
@@ -459,7 +468,7 @@ __global__ void __launch_bounds__(256) k_hsmac_faces(Ctx* __restrict__ ctx, Grid
   T* W = (T*)ctx->vel[set][2];
   const T dxi = (T)cf.dxi, dyi = (T)cf.dyi, dzi = (T)cf.dzi, dl = (T)cf.dl, om = (T)cf.omega;
   const T dti = (T)(1.0 / ctx->scal[0]);
-  const int stride = gridDim.x * blockDim.x;
+  const int stride = (int)nb * blockDim.x;
   double acc = 0.0;
   bool ok = true;
   for (int p = 0; p < 6; p++) {
@@ -476,7 +485,7 @@ __global__ void __launch_bounds__(256) k_hsmac_faces(Ctx* __restrict__ ctx, Grid
     // Loads bypass L1 (__ldcg): after a grid barrier a block reads cells that
     // other blocks have just written.
     constexpr int KB = 4;
-    for (int t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < nt; t0 += KB * stride) {
+    for (int t0 = (int)bid * blockDim.x + threadIdx.x; t0 < nt; t0 += KB * stride) {
       int64_t c[KB];
       bool v[KB], inr[KB];
       T u0[KB], u1[KB], v0[KB], v1[KB], w0[KB], w1[KB], p0[KB];
@@ -515,16 +524,16 @@ __global__ void __launch_bounds__(256) k_hsmac_faces(Ctx* __restrict__ ctx, Grid
         if (inr[q]) acc += (double)div * (double)div;
       }
     }
-    if (p < 5 && !grid_barrier(ctx, gridDim.x, &flag)) {
+    if (p < 5 && !grid_barrier(ctx, nb, &flag)) {
       if (threadIdx.x == 0) ctx->wait_error = 1;
       ok = false;
       break;
     }
   }
   const double s = block_sum<256>(acc, sh);
-  if (threadIdx.x == 0) partials[part0 + blockIdx.x] = s;
-  if (last_block(&ctx->ticket, gridDim.x, &flag)) {
-    const double tot = sum_partials<256>(partials, part0 + (int)gridDim.x, sh);
+  if (threadIdx.x == 0) partials[part0 + bid] = s;
+  if (last_block(&ctx->ticket, nb, &flag)) {
+    const double tot = sum_partials<256>(partials, part0 + (int)nb, sh);
     if (threadIdx.x == 0) {
       ctx->ticket = 0;
       ctx->gbar_count = 0;  // every block has left its last barrier
@@ -536,6 +545,33 @@ __global__ void __launch_bounds__(256) k_hsmac_faces(Ctx* __restrict__ ctx, Grid
       }
     }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_hsmac_faces(Ctx* __restrict__ ctx, Grid g, int set, T* __restrict__ P,
+                                                     FaceSet fs, HsmacCoef cf, double* __restrict__ partials,
+                                                     int part0, int group_end) {
+  hsmac_faces_body<T>(ctx, g, set, P, fs, cf, partials, part0, group_end, blockIdx.x, gridDim.x);
+}
+
+// Per-handle pointers of a batch group (one handle per blockIdx.y).
+constexpr int kGroupPtrMax = 64;
+template <typename T>
+struct GroupPtrs {
+  Ctx* ctx[kGroupPtrMax];
+  T* P[kGroupPtrMax];
+  double* partials[kGroupPtrMax];
+};
+template <typename T>
+__global__ void __launch_bounds__(256) k_hsmac_faces_group(const __grid_constant__ GroupPtrs<T> ga, Grid g, int set,
+                                                           FaceSet fs, HsmacCoef cf, int part0, int group_end) {
+  const int m = blockIdx.y;
+  hsmac_faces_body<T>(ga.ctx[m], g, set, ga.P[m], fs, cf, ga.partials[m], part0, group_end, blockIdx.x, gridDim.x);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_fill_halo_group(const __grid_constant__ GroupPtrs<T> ga, Grid g, FillArgs fa,
+                                                         int r, int full, int64_t total) {
+  fill_halo_body<T>(ga.ctx[blockIdx.y], g, fa, r, full, total);
 }
 
 // Fused red-black sweep over the box D with the velocities ping-ponged:
@@ -779,6 +815,14 @@ __global__ void k_couple_log(Ctx* ctx, int stage) {
 // WHILE-node condition of the device-resident couple loop.
 __global__ void k_couple_continue(const Ctx* ctx, cudaGraphConditionalHandle handle) {
   cudaGraphSetConditional(handle, ctx->cs.cont ? 1u : 0u);
+}
+// the group's loop goes on while any member's does (done members' blocks
+// return at once in every group launch)
+template <typename T>
+__global__ void k_group_continue(const __grid_constant__ GroupPtrs<T> ga, int m, cudaGraphConditionalHandle handle) {
+  unsigned int c = 0;
+  for (int q = 0; q < m; q++) c |= ga.ctx[q]->cs.cont ? 1u : 0u;
+  cudaGraphSetConditional(handle, c);
 }
 
 // --------------------------------------------------------------------------

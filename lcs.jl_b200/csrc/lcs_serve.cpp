@@ -56,16 +56,39 @@ struct lcs_batch {
   std::vector<lcs_handle*> members;
   std::vector<lcs_config> cfgs;
   std::vector<MemberTuning> tuning;
+  std::vector<lcs_group*> groups;          // members stepped as one graph (lcs_group_*)
+  std::vector<std::vector<int32_t>> group_members;
+  std::vector<int32_t> group_of;           // member -> index in groups, or -1
 };
 
 namespace {
 
+bool grouping_enabled() {
+  const char* g = std::getenv("LCS_BATCH_GROUP");
+  return !(g && std::string(g) == "0");
+}
+
+// Steps one batch of handles once (a group when there is one) and waits.
+bool probe_step(const std::vector<lcs_handle*>& probes, lcs_group* pg) {
+  bool ok = true;
+  size_t begun = 0;
+  if (pg) {
+    ok = lcs_group_step_begin(pg, 1) == LCS_OK;
+    begun = ok ? probes.size() : 0;
+  } else {
+    for (; begun < probes.size() && ok; begun++) ok = lcs_step_begin(probes[begun], 1) == LCS_OK;
+  }
+  for (size_t q = 0; q < begun; q++) ok = lcs_step_finish(probes[q], nullptr) == LCS_OK && ok;
+  return ok;
+}
+
 // The batch's autotuner.  Members that share a shape (dims and precision) get
 // the same launch shapes: for every candidate (tile rows of the sweep x z
-// chunk) it steps probe handles of that shape, one per member, together (zero
-// fields, exactly 20 sweeps per couple, no particles) and times one step; the
-// fastest candidate is applied to the members.  Probes never touch a member's
-// state, and no result depends on the launch shapes.
+// chunk x the part of the GPU a launch is sized for) it steps probe handles of
+// that shape, one per member, together (as one group when grouping is on;
+// zero fields, exactly 20 sweeps per couple, no particles) and times one
+// step; the fastest candidate is applied to the members.  Probes never touch
+// a member's state, and no result depends on the launch shapes.
 int autotune(lcs_batch* b) {
   const size_t m = b->members.size();
   double total_cells = 0.0;
@@ -103,6 +126,10 @@ int autotune(lcs_batch* b) {
       }
       probes.push_back(h);
     }
+    lcs_group* pg = nullptr;
+    if (grouping_enabled() && probes.size() >= 2 && probes.size() <= 64 &&
+        lcs_group_create(probes.data(), (int32_t)probes.size(), &pg) != LCS_OK)
+      pg = nullptr;
     MemberTuning best;
     best.share = share;
     best.probe_ms = 1e300;
@@ -115,20 +142,21 @@ int autotune(lcs_batch* b) {
     // for the whole GPU, or a fixed chunk)
     struct Cand { int32_t rows, zc; double share; };
     std::vector<Cand> cands;
+    // a grouped launch covers every member of the shape: each member's share of it
+    const double share_m = std::max(1e-3, share / (double)std::max<size_t>(1, group.size()));
     for (int32_t rows : rows_c) {
       cands.push_back({rows, 0, share});
       cands.push_back({rows, 0, 1.0});
+      if (pg) cands.push_back({rows, 0, share_m});
       for (int32_t zc : zc_c)
-        if (zc > 0) cands.push_back({rows, zc, share});
+        if (zc > 0) cands.push_back({rows, zc, pg ? share_m : share});
     }
     for (const Cand& cd : cands) {
       bool ok = !probes.empty();
       for (lcs_handle* h : probes) ok = ok && lcs_set_tuning(h, cd.rows, cd.zc, cd.share) == LCS_OK;
       for (int rep = 0; ok && rep < 2; rep++) {  // rep 0 captures the graphs; rep 1 is timed
         const auto t0 = Clock::now();
-        size_t begun = 0;
-        for (; begun < probes.size() && ok; begun++) ok = lcs_step_begin(probes[begun], 1) == LCS_OK;
-        for (size_t q = 0; q < begun; q++) ok = lcs_step_finish(probes[q], nullptr) == LCS_OK && ok;
+        ok = probe_step(probes, pg);
         const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
         if (ok && rep == 1 && ms < best.probe_ms) {
           best.rw_rows = cd.rows;
@@ -138,6 +166,7 @@ int autotune(lcs_batch* b) {
         }
       }
     }
+    if (pg) lcs_group_destroy(pg);
     for (lcs_handle* h : probes) lcs_destroy(h);
     if (best.probe_ms >= 1e300) {  // no probe could run: the built-in shapes
       best.rw_rows = 0;
@@ -161,6 +190,41 @@ int autotune(lcs_batch* b) {
 // the queues to the maximum (32) only when no context exists yet and the user
 // has not chosen a value.
 void widen_work_queues() { setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0); }
+
+// Members with the same dims, precision and launch shapes step as groups of
+// up to 64 (lcs_group_create checks the rest: halo and HSMAC settings); a
+// member no group accepts steps alone.
+void make_groups(lcs_batch* b) {
+  const size_t m = b->members.size();
+  b->group_of.assign(m, -1);
+  if (!grouping_enabled()) return;
+  std::vector<bool> done(m, false);
+  for (size_t i = 0; i < m; i++) {
+    if (done[i]) continue;
+    std::vector<int32_t> same;
+    for (size_t q = i; q < m; q++) {
+      const lcs_config &a = b->cfgs[i], &c = b->cfgs[q];
+      const MemberTuning &ta = b->tuning[i], &tc = b->tuning[q];
+      if (!done[q] && a.dims[0] == c.dims[0] && a.dims[1] == c.dims[1] && a.dims[2] == c.dims[2] &&
+          a.precision == c.precision && ta.rw_rows == tc.rw_rows && ta.zchunk == tc.zchunk && ta.share == tc.share) {
+        same.push_back((int32_t)q);
+        done[q] = true;
+      }
+    }
+    for (size_t c0 = 0; c0 + 1 < same.size(); c0 += 64) {
+      const size_t cn = std::min<size_t>(64, same.size() - c0);
+      if (cn < 2) break;
+      std::vector<lcs_handle*> hs;
+      for (size_t q = 0; q < cn; q++) hs.push_back(b->members[same[c0 + q]]);
+      lcs_group* g = nullptr;
+      if (lcs_group_create(hs.data(), (int32_t)cn, &g) != LCS_OK) continue;
+      const int32_t gi = (int32_t)b->groups.size();
+      b->groups.push_back(g);
+      b->group_members.emplace_back(same.begin() + c0, same.begin() + c0 + cn);
+      for (size_t q = 0; q < cn; q++) b->group_of[same[c0 + q]] = gi;
+    }
+  }
+}
 
 }  // namespace
 
@@ -196,6 +260,7 @@ int lcs_batch_create(const lcs_config* members, int32_t m, lcs_batch** out) {
       return rc;
     }
   }  // else: the built-in shapes of a solo run
+  make_groups(b.get());
   *out = b.release();
   return LCS_OK;
 }
@@ -234,16 +299,28 @@ int lcs_batch_step(lcs_batch* b, int32_t nsteps, lcs_log* logs) {
     const int32_t chunk = std::min<int32_t>(nsteps - done, LCS_MAX_ASYNC_STEPS);
     int first_rc = LCS_OK;
     std::string first_err;
-    int32_t begun = 0;
-    for (; begun < m; begun++) {  // enqueue every member before waiting for any
-      const int rc = lcs_step_begin(b->members[begun], chunk);
+    std::vector<char> begun(m, 0);
+    for (size_t gi = 0; gi < b->groups.size() && first_rc == LCS_OK; gi++) {  // enqueue everything first
+      const int rc = lcs_group_step_begin(b->groups[gi], chunk);
       if (rc != LCS_OK) {
         first_rc = rc;
-        first_err = "batch member " + std::to_string(begun) + ": " + handle_error(b->members[begun]);
-        break;
+        first_err = "batch group " + std::to_string(gi) + ": " + handle_error(nullptr);
+      } else {
+        for (int32_t q : b->group_members[gi]) begun[q] = 1;
       }
     }
-    for (int32_t i = 0; i < begun; i++) {
+    for (int32_t i = 0; i < m && first_rc == LCS_OK; i++) {
+      if (b->group_of[i] >= 0) continue;
+      const int rc = lcs_step_begin(b->members[i], chunk);
+      if (rc != LCS_OK) {
+        first_rc = rc;
+        first_err = "batch member " + std::to_string(i) + ": " + handle_error(b->members[i]);
+      } else {
+        begun[i] = 1;
+      }
+    }
+    for (int32_t i = 0; i < m; i++) {
+      if (!begun[i]) continue;
       const int rc = lcs_step_finish(b->members[i], logs ? logs + (size_t)i * nsteps + done : nullptr);
       if (rc != LCS_OK && first_rc == LCS_OK) {
         first_rc = rc;
@@ -258,6 +335,7 @@ int lcs_batch_step(lcs_batch* b, int32_t nsteps, lcs_log* logs) {
 
 void lcs_batch_destroy(lcs_batch* b) {
   if (!b) return;
+  for (lcs_group* g : b->groups) lcs_group_destroy(g);
   for (lcs_handle* h : b->members) lcs_destroy(h);
   delete b;
 }

@@ -248,6 +248,9 @@ PROTOTYPES = {
                                      C.POINTER(ParticleStats)]),
     "lcs_particles_density": (C.c_int, [_P, C.c_int32, C.c_int32, _D]),
     "lcs_upload_flow_coarse": (C.c_int, [_P, _D, _D, _D, _D]),
+    "lcs_group_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
+    "lcs_group_step_begin": (C.c_int, [_P, C.c_int32]),
+    "lcs_group_destroy": (None, [_P]),
     "lcs_step_begin": (C.c_int, [_P, C.c_int32]),
     "lcs_step_poll": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "lcs_step_finish": (C.c_int, [_P, C.POINTER(Log)]),

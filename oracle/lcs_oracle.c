@@ -1008,6 +1008,44 @@ int lcs_upload_flow_coarse(lcs_handle* h, const double* U, const double* V, cons
   return LCS_OK;
 }
 
+/* Groups (no reference counterpart): on the CPU a group's step is its members'
+ * steps one after another. */
+struct lcs_group {
+  int32_t m;
+  lcs_handle** h;
+};
+int lcs_group_create(lcs_handle* const* members, int32_t m, lcs_group** out) {
+  if (!out) return fail(NULL, LCS_EINVAL, "null output");
+  *out = NULL;
+  if (!members || m < 2 || m > 64) return fail(NULL, LCS_EINVAL, "a group has 2..64 members");
+  for (int32_t q = 0; q < m; q++) {
+    if (!members[q]) return fail(NULL, LCS_EINVAL, "null group member");
+    const lcs_config *a = &members[0]->cfg, *b = &members[q]->cfg;
+    if (a->dims[0] != b->dims[0] || a->dims[1] != b->dims[1] || a->dims[2] != b->dims[2] ||
+        a->halo_size != b->halo_size || a->precision != b->precision || a->itrmax != b->itrmax)
+      return fail(NULL, LCS_EINVAL, "group members differ in shape or HSMAC settings");
+  }
+  lcs_group* g = (lcs_group*)calloc(1, sizeof *g);
+  g->m = m;
+  g->h = (lcs_handle**)calloc((size_t)m, sizeof *g->h);
+  memcpy(g->h, members, (size_t)m * sizeof *g->h);
+  *out = g;
+  return LCS_OK;
+}
+int lcs_group_step_begin(lcs_group* g, int32_t nsteps) {
+  if (!g) return fail(NULL, LCS_EINVAL, "null group");
+  for (int32_t q = 0; q < g->m; q++) {
+    const int rc = lcs_step_begin(g->h[q], nsteps);
+    if (rc) return fail(NULL, rc, "group member %d: %s", q, g->h[q]->err);
+  }
+  return LCS_OK;
+}
+void lcs_group_destroy(lcs_group* g) {
+  if (!g) return;
+  free(g->h);
+  free(g);
+}
+
 int lcs_download_flow(lcs_handle* h, double* U, double* V, double* W, double* P) {
   int rc = 0;
   if (U) rc |= lcs_field_get(h, LCS_FIELD_U, U, 0);

@@ -44,6 +44,61 @@ def member_configs(precision=F.PRECISION_FP64):
     ]
 
 
+def group_configs(precision=F.PRECISION_FP64, n=24, count=4):
+    """Members of one shape (the grouped form): different viscosity, forcing,
+    particle counts and species; same dims, halo and HSMAC settings."""
+    kinds = [
+        dict(species=[{"n": 300, "density_ratio": 843.0}], Re=80.0),
+        dict(species=[{"n": 120, "density_ratio": 100.0}, {"n": 200, "density_ratio": 843.0}],
+             forcing=F.FORCING_LINEAR_POWER, power=0.5, Re=60.0),
+        dict(mode=F.MODE_FLOW, Re=40.0),
+        dict(species=[{"n": 500, "density_ratio": 843.0}], forcing=F.FORCING_LINEAR_POWER, power=0.3, Re=120.0),
+    ]
+    return [make_config(n, itrmax=8, precision=precision, **kinds[i % len(kinds)]) for i in range(count)]
+
+
+def load_inputs(e, cfg, seed):
+    flow, parts = inputs(cfg, seed)
+    e.upload_flow(*flow)
+    for s, p in enumerate(parts):
+        e.upload_particles(s, p["diam"], p["x"], p["y"], p["z"], p["u"], p["v"], p["w"])
+        e.init_particle_velocity(s)
+
+
+def check_group_equals_members_alone(engine_cls, lib, precision=F.PRECISION_FP64, count=4, nsteps=3, n=24):
+    """lcs_group_create over handles of one shape: each member's fields,
+    particles and logs equal the member stepped alone, bit for bit."""
+    import ctypes as C
+
+    cfgs = group_configs(precision, n=n, count=count)
+    engines = [engine_cls(c) for c in cfgs]
+    for i, (c, e) in enumerate(zip(cfgs, engines)):
+        load_inputs(e, c, 200 + i)
+    hs = (C.c_void_p * count)(*[e.handle.value for e in engines])
+    grp = C.c_void_p()
+    assert lib.lcs_group_create(hs, count, C.byref(grp)) == 0, lib.lcs_last_error(None)
+    logs = []
+    for rep in range(2):  # the second round replays the captured group graph
+        assert lib.lcs_group_step_begin(grp, nsteps) == 0, lib.lcs_last_error(None)
+        for e in engines:
+            lg = (_abi.Log * nsteps)()
+            e._check(lib.lcs_step_finish(e.handle, lg))
+            if rep == 1:
+                logs.append([x.as_dict() for x in lg])
+    lib.lcs_group_destroy(grp)
+    for i, (c, e) in enumerate(zip(cfgs, engines)):
+        c.use_graphs = 1
+        flow, parts, ref_logs = run_alone(engine_cls, c, 200 + i, 2 * nsteps)
+        assert same_logs(logs[i], ref_logs[nsteps:]), i
+        for a, r in zip(e.download_flow(), flow):
+            assert np.array_equal(a, r), i
+        for s in range(len(parts)):
+            got = e.download_particles(s)
+            for k in ("x", "y", "z", "u", "v", "w"):
+                assert np.array_equal(got[k], parts[s][k]), (i, s, k)
+        e.close()
+
+
 def inputs(cfg, seed):
     """Seeded initial state of one run: interior fields and particle species."""
     nx, ny, nz = (int(d) for d in cfg.dims)
@@ -104,8 +159,8 @@ def check_async_equals_step(engine_cls, lib):
     e.close()
 
 
-def check_batch_equals_members_alone(engine_cls, lib, precision=F.PRECISION_FP64, nsteps=3):
-    cfgs = member_configs(precision)
+def check_batch_equals_members_alone(engine_cls, lib, precision=F.PRECISION_FP64, nsteps=3, cfgs=None):
+    cfgs = member_configs(precision) if cfgs is None else cfgs
     b = Batch(cfgs, lib=lib)
     for i, (cfg, e) in enumerate(zip(cfgs, b.members)):
         flow, parts = inputs(cfg, 100 + i)

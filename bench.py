@@ -68,6 +68,8 @@ WORKLOADS = {
 # `python bench.py --steps 1 --warmup 0 --no-cpu-baseline` (rc256), averaged:
 # 1135.9 MB and 1200.2 MB per launch over 256^3 cells.
 SWEEP_DRAM_BYTES_PER_CELL = {"hsmac_rw": 69.6}
+# the FP32 form: 588.8 MB and 629.6 MB per launch (profiles/hsmac_rw_fp32_rc256.md)
+SWEEP_DRAM_BYTES_PER_CELL_FP32 = {"hsmac_rw": 36.3}
 SWEEP_KERNELS = ("hsmac_rw", "hsmac_tma", "hsmac_fused")
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -307,12 +309,12 @@ def run_b200(args):
     # the dominant kernel: the fused red-black sweep (TMA-fed, or the plain form)
     sweep_kernel = max(SWEEP_KERNELS, key=lambda k: tot.get(k, (0.0, 0))[0])
     ms_sweep, cnt = tot.get(sweep_kernel, (0.0, 0))
-    T = 8
+    T = 4 if args.precision == "fp32-mixed" else 8  # bytes per field element
     peak, peak_kind = hbm_peak()
     alg_bytes = 8 * T * n3  # U, V, W, P read and written once per interior cell per sweep
     avg_ms = ms_sweep / max(cnt, 1)
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9 if cnt else None
-    traffic = SWEEP_DRAM_BYTES_PER_CELL.get(sweep_kernel)
+    traffic = (SWEEP_DRAM_BYTES_PER_CELL_FP32 if T == 4 else SWEEP_DRAM_BYTES_PER_CELL).get(sweep_kernel)
     traffic = traffic * n3 if traffic else None
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in sorted(tot.items(), key=lambda kv: -kv[1][0])}
 

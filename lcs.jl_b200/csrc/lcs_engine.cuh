@@ -26,6 +26,7 @@
 #include "lcs_kernels.cuh"
 #include "lcs_hsmac_tma.cuh"
 #include "lcs_hsmac_rw.cuh"
+#include "lcs_hsmac_rw4.cuh"
 #include "lcs_makeindex.cuh"
 #include "lcs_pstat.cuh"
 
@@ -377,6 +378,8 @@ class Engine : public EngineBase {
         const std::string t(v);
         rw_variant = t == "8" ? 1 : t == "5" ? 2 : 0;
       }
+      const char* q4 = std::getenv("LCS_B200_RW4");
+      use_rw4 = std::is_same<T, float>::value && q4 && std::string(q4) == "1";
       LCS_TRY(init_rw_maps());
     }
     return LCS_OK;
@@ -384,6 +387,9 @@ class Engine : public EngineBase {
   // The row-warp sweep of the current rw_variant: kernel, shared memory,
   // occupancy and its tensor maps (box 64 x rows+4 and 64 x rows).
   int init_rw_maps() {
+    if constexpr (std::is_same<T, float>::value) {
+      if (use_rw4) return init_rw4_maps();
+    }
     switch (rw_variant) {
       case 1: RTY = 8; rw_smem = RwLayout<T, 8, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 8, 3>;
               rw_threads = RwLayout<T, 8, 3>::NT; break;
@@ -419,6 +425,39 @@ class Engine : public EngineBase {
     if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the row-warp sweep does not fit on an SM");
     return LCS_OK;
   }
+  // the quad sweep's kernels and tensor maps (box 128 x rows+4 and 128 x rows)
+  int init_rw4_maps() {
+    const void* grp_fn = nullptr;
+    switch (rw_variant) {
+      case 1: RTY = 8; rw_smem = Rw4Layout<8, 3>::total; rw_fn = (const void*)k_hsmac_rw4<8, 3>;
+              grp_fn = (const void*)k_hsmac_rw4_group<8, 3>; rw_threads = Rw4Layout<8, 3>::NT; break;
+      case 2: RTY = 5; rw_smem = Rw4Layout<5, 3>::total; rw_fn = (const void*)k_hsmac_rw4<5, 3>;
+              grp_fn = (const void*)k_hsmac_rw4_group<5, 3>; rw_threads = Rw4Layout<5, 3>::NT; break;
+      default: RTY = 13; rw_smem = Rw4Layout<13, 3>::total; rw_fn = (const void*)k_hsmac_rw4<13, 3>;
+               grp_fn = (const void*)k_hsmac_rw4_group<13, 3>; rw_threads = Rw4Layout<13, 3>::NT; break;
+    }
+    const CUtensorMapDataType dtype = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)(g.n[1] + 2 * g.h), (cuuint64_t)(g.n[2] + 2 * g.h)};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.pz * sizeof(T)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const cuuint32_t rbox[3] = {(cuuint32_t)RW4_W, (cuuint32_t)RTY + 4, 1};
+    for (int b = 0; b < kVelMaps; b++) {
+      CUresult rr = encode_fn(&tmaps_rw4.vel[b], dtype, 3, vel0[b / 3][b % 3], dims, strides, rbox, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (rr != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (quad velocity %d) failed: %d", b, (int)rr);
+    }
+    const cuuint32_t rpbox[3] = {(cuuint32_t)RW4_W, (cuuint32_t)RTY, 1};
+    CUresult rp = encode_fn(&tmaps_rw4.P, dtype, 3, (void*)P, dims, strides, rpbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (rp != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (quad P) failed: %d", (int)rp);
+    LCS_CUDA(cudaFuncSetAttribute(rw_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
+    LCS_CUDA(cudaFuncSetAttribute(grp_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
+    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rw_ctas_per_sm, rw_fn, rw_threads, rw_smem));
+    if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the quad row-warp sweep does not fit on an SM");
+    return LCS_OK;
+  }
   PFN_cuTensorMapEncodeTiled_v12000 encode_fn = nullptr;
   int num_sms = 148, tma_ctas_per_sm = 1;
   bool use_rw = false;
@@ -426,6 +465,11 @@ class Engine : public EngineBase {
   int rw_variant = 0, RTY = 13, rw_threads = 512, rw_ctas_per_sm = 1;
   size_t rw_smem = 0;
   const void* rw_fn = nullptr;
+  // FP32: the quad row-warp sweep (four cells per lane, tiles 120 wide),
+  // chosen by LCS_B200_RW4=1; measured slower than the pair sweep at 256^3
+  // (226 vs 213 us per sweep), so the pair sweep is the default
+  bool use_rw4 = false;
+  TensorMaps tmaps_rw4;
 
   // blocks of the cooperative face-phase kernel (0: twelve in-place launches)
   int face_grid = 0;
@@ -678,6 +722,9 @@ class Engine : public EngineBase {
   int fused_rw(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
     if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
     const Box gb = bbox(out, cube(g, 1, 0));
+    if constexpr (std::is_same<T, float>::value) {
+      if (use_rw4) return fused_rw4(set, D, out, gb, part, finalize, group_end, nblocks);
+    }
     // first tile column: the largest x0 <= gb.lo[0] with x0-2 on a 16-byte
     // boundary (x0 odd in FP64, x0 = 3 mod 4 in FP32); tiles step by RW_TX = 60
     const int am = 16 / (int)sizeof(T), ar = am - 1;
@@ -698,6 +745,54 @@ class Engine : public EngineBase {
                             out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
       default: return launch("hsmac_rw", k_hsmac_rw<T, 13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P,
                              D, out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
+    }
+  }
+  // FP32 quad sweep: tiles of RW4_TX x RTY whose first column x0 = 1 mod 4
+  // (x0-4 on a 16-byte boundary)
+  int fused_rw4(int set, Box D, Box out, Box gb, double* part, int finalize, int group_end, int* nblocks) {
+    int xo = gb.lo[0];
+    while (((xo % 4) + 4) % 4 != 1) xo--;
+    const int gx = (gb.hi[0] - xo + 1 + RW4_TX - 1) / RW4_TX, gy = (gb.len(1) + RTY - 1) / RTY;
+    const int nzc = gb.len(2), ncols = gx * gy;
+    const RwSched sc = rw_schedule(ncols, nzc, num_sms * rw_ctas_per_sm);
+    if (sc.nitems > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
+    if (nblocks) *nblocks = sc.nitems;
+    if (grp) {
+      const int M = (int)grp->size();
+      for (int m0 = 0; m0 < M; m0 += kGroupMax) {
+        const int mc = std::min(kGroupMax, M - m0);
+        GroupRwArgs<float> ga;
+        memset(&ga, 0, sizeof ga);
+        for (int q = 0; q < mc; q++) {
+          Engine<T>* e = (*grp)[m0 + q];
+          ga.tm[q] = e->tmaps_rw4;
+          ga.ctx[q] = e->dctx;
+          ga.P[q] = (float*)e->P;
+          ga.partials[q] = e->partials;
+        }
+        const dim3 grid(sc.nitems, mc), block(rw_threads);
+        int rc2;
+        switch (rw_variant) {
+          case 1: rc2 = launch("hsmac_rw", k_hsmac_rw4_group<8, 3>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
+                               gx, gy, sc, hc, finalize, group_end); break;
+          case 2: rc2 = launch("hsmac_rw", k_hsmac_rw4_group<5, 3>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
+                               gx, gy, sc, hc, finalize, group_end); break;
+          default: rc2 = launch("hsmac_rw", k_hsmac_rw4_group<13, 3>, grid, block, rw_smem, ga, g, set, D, out, gb,
+                                xo, gx, gy, sc, hc, finalize, group_end);
+        }
+        LCS_TRY(rc2);
+      }
+      return LCS_OK;
+    }
+    const dim3 grid(sc.nitems), block(rw_threads);
+    float* Pf = (float*)P;
+    switch (rw_variant) {
+      case 1: return launch("hsmac_rw", k_hsmac_rw4<8, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw4, Pf, D, out,
+                            gb, xo, gx, gy, sc, hc, part, finalize, group_end);
+      case 2: return launch("hsmac_rw", k_hsmac_rw4<5, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw4, Pf, D, out,
+                            gb, xo, gx, gy, sc, hc, part, finalize, group_end);
+      default: return launch("hsmac_rw", k_hsmac_rw4<13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw4, Pf, D,
+                             out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
     }
   }
   // the same sweep for every member of the group, kGroupMax members a launch
@@ -2051,7 +2146,8 @@ int Engine<T>::group_create(EngineBase* const* members, int m, GroupBase** out) 
                       a.omega == b.omega && a.epsp == b.epsp && a.itrmin == b.itrmin && a.itrmax == b.itrmax;
     if (!same) return fail(LCS_EINVAL, "group members differ in shape or HSMAC settings");
     if (!e->use_rw) return fail(LCS_EINVAL, "group members need the row-warp sweep");
-    if (e->rw_variant != L->rw_variant || e->zchunk_force != L->zchunk_force || e->sm_share != L->sm_share)
+    if (e->rw_variant != L->rw_variant || e->zchunk_force != L->zchunk_force || e->sm_share != L->sm_share ||
+        e->use_rw4 != L->use_rw4)
       return fail(LCS_EINVAL, "group members differ in launch shapes");
     if (e->async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on a member");
     if (e->face_grid <= 0) return fail(LCS_EINVAL, "group members need the cooperative face kernel");

@@ -147,6 +147,8 @@ typedef struct lcs_handle lcs_handle;
 LCS_API int lcs_create(const lcs_config* cfg, lcs_handle** out);
 LCS_API void lcs_destroy(lcs_handle* h);
 LCS_API const char* lcs_last_error(const lcs_handle* h);
+/* The configuration the handle was created with. */
+LCS_API int lcs_get_config(const lcs_handle* h, lcs_config* out);
 /* Bytes of device memory the handle holds (the serving admission uses it). */
 LCS_API int lcs_footprint(const lcs_config* cfg, int64_t* bytes);
 
@@ -299,6 +301,30 @@ LCS_API int lcs_particles_stat(lcs_handle* h, int32_t species, const lcs_particl
  * 27 neighbouring cells with h = min spacing; densities[nvalid] in the new
  * device order (0 for a particle outside the cell domain). */
 LCS_API int lcs_particles_density(lcs_handle* h, int32_t species, int32_t grid_ratio, double* densities);
+
+/* ---- restart files (src/LCSIO/save.jl:40-167, load.jl:23-118) ------------
+ * The reference's restart layout in HDF5 (written and read without an HDF5
+ * library, for the subset these files use: version 0 superblock, symbol-table
+ * groups, contiguous little-endian F64/I64 datasets):
+ *   /flow/{U,V,W,P}                        Float64 (nz, ny, nx), the interiors
+ *   /particles/<s+1>/counts                Int64 (1,) = nvalid
+ *   /particles/<s+1>/{id,x,y,z,u,v,w,diam} Int64 / Float64 (nvalid,)
+ * lcs_restart_load reads such a file into the handle (its dims and particle
+ * counts must match, as load.jl checks); lcs_restart_load_coarse reads the
+ * flow of a restart with half the dims and upsamples it (the `upsample` init,
+ * src/LCSIO/upsample.jl:1-45).  lcs_stat_state_save/load write and read the
+ * `<step>/state/{step,t,dt}` entries of a stat file (save.jl:17-31, the resume
+ * of load.jl:1-21).  lcs_h5_dataset / lcs_h5_list inspect any file of the
+ * subset.  Errors: LCS_EINVAL with lcs_io_last_error(). */
+LCS_API int lcs_restart_save(lcs_handle* h, const char* path);
+LCS_API int lcs_restart_load(lcs_handle* h, const char* path);
+LCS_API int lcs_restart_load_coarse(lcs_handle* h, const char* path);
+LCS_API int lcs_stat_state_save(const char* path, int64_t step, double t, double dt);
+LCS_API int lcs_stat_state_load(const char* path, int64_t step, double* t, double* dt);
+LCS_API int lcs_h5_dataset(const char* path, const char* name, int32_t* rank, int64_t* dims, char* kind, void* buf,
+                           int64_t bytes);
+LCS_API int lcs_h5_list(const char* path, const char* group, char* buf, int64_t cap);
+LCS_API const char* lcs_io_last_error(void);
 
 /* ---- asynchronous steps (no reference counterpart) ----------------------
  * For hosts that drive many handles at once (the batching and serving forms

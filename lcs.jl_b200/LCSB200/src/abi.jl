@@ -150,3 +150,11 @@ function particle_density(h, s, grid_ratio, n)
         h, s, grid_ratio, rho))
     rho
 end
+
+# ---- restart files (the reference's HDF5 layout, read and written by the library)
+ioerror() = unsafe_string(ccall((:lcs_io_last_error, LIB), Cstring, ()))
+checkio(rc) = rc == 0 || throw(ArgumentError("lcs_b200: " * ioerror()))
+restart_save(h, path::AbstractString) = checkio(ccall((:lcs_restart_save, LIB), Cint, (Ptr{Cvoid}, Cstring), h, path))
+restart_load!(h, path::AbstractString) = checkio(ccall((:lcs_restart_load, LIB), Cint, (Ptr{Cvoid}, Cstring), h, path))
+restart_load_coarse!(h, path::AbstractString) =
+    checkio(ccall((:lcs_restart_load_coarse, LIB), Cint, (Ptr{Cvoid}, Cstring), h, path))

@@ -126,6 +126,12 @@ void lcs_destroy(lcs_handle* h) {
 
 const char* lcs_last_error(const lcs_handle* h) { return h ? h->e->err.c_str() : g_err; }
 
+int lcs_get_config(const lcs_handle* h, lcs_config* out) {
+  if (!h || !out) return set_global_error(LCS_EINVAL, "null argument");
+  *out = h->e->config();
+  return LCS_OK;
+}
+
 #define H(h) \
   if (!(h)) return set_global_error(LCS_EINVAL, "null handle");
 

@@ -1432,6 +1432,7 @@ class Engine : public EngineBase {
     return LCS_OK;
   }
   int group_create(EngineBase* const* members, int m, GroupBase** out) override;
+  const lcs_config& config() const override { return cfg; }
   int step_poll(int* done) override {
     if (!done) return fail(LCS_EINVAL, "null output");
     if (!async_pending) return fail(LCS_ESTATE, "no steps in flight on this handle");

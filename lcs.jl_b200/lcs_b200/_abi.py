@@ -251,6 +251,16 @@ PROTOTYPES = {
     "lcs_group_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
     "lcs_group_step_begin": (C.c_int, [_P, C.c_int32]),
     "lcs_group_destroy": (None, [_P]),
+    "lcs_get_config": (C.c_int, [_P, C.POINTER(Config)]),
+    "lcs_restart_save": (C.c_int, [_P, C.c_char_p]),
+    "lcs_restart_load": (C.c_int, [_P, C.c_char_p]),
+    "lcs_restart_load_coarse": (C.c_int, [_P, C.c_char_p]),
+    "lcs_stat_state_save": (C.c_int, [C.c_char_p, C.c_int64, C.c_double, C.c_double]),
+    "lcs_stat_state_load": (C.c_int, [C.c_char_p, C.c_int64, _D, _D]),
+    "lcs_h5_dataset": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int32), _I64, C.c_char_p, C.c_void_p,
+                                 C.c_int64]),
+    "lcs_h5_list": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int64]),
+    "lcs_io_last_error": (C.c_char_p, []),
     "lcs_step_begin": (C.c_int, [_P, C.c_int32]),
     "lcs_step_poll": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "lcs_step_finish": (C.c_int, [_P, C.POINTER(Log)]),

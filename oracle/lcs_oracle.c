@@ -914,6 +914,12 @@ void lcs_destroy(lcs_handle* h) {
 
 const char* lcs_last_error(const lcs_handle* h) { return h ? h->err : g_err; }
 
+int lcs_get_config(const lcs_handle* h, lcs_config* out) {
+  if (!h || !out) return LCS_EINVAL;
+  *out = h->cfg;
+  return LCS_OK;
+}
+
 static double* field_ptr(lcs_handle* h, int f) {
   switch (f) {
     case LCS_FIELD_U: return h->U;

@@ -1,0 +1,155 @@
+"""Restart files in the reference's HDF5 layout (src/LCSIO/save.jl:40-167,
+load.jl:23-118) through the library's own reader and writer, over the CPU
+oracle (the I/O is host code over the public ABI, linked into both libraries).
+
+The reader is checked against a file written by the HDF5 library itself: the
+MATLAB 7.3 test file that SciPy ships (a 512-byte user block, then HDF5 with
+libhdf5's own layout), whose `testdouble` is pi * [0..8] / 4.  The writer uses
+the same encodings, compared byte for byte where the two overlap.
+"""
+
+import math
+import os
+import struct
+
+import numpy as np
+import pytest
+
+from helpers import make_config
+from lcs_b200 import _abi, restart
+from oracle_engine import OracleEngine, load_oracle
+
+
+def libhdf5_file():
+    import scipy
+
+    p = os.path.join(os.path.dirname(scipy.__file__), "io", "matlab", "tests", "data", "testhdf5_7.4_GLNX86.mat")
+    if not os.path.exists(p):
+        pytest.skip("the SciPy HDF5 test file is not installed")
+    return p
+
+
+def test_reads_a_file_written_by_libhdf5():
+    lib = load_oracle()
+    p = libhdf5_file()
+    assert restart.listing(lib, p) == ["testdouble"]
+    a = restart.dataset(lib, p, "testdouble")
+    assert a.shape == (9, 1)
+    assert np.allclose(a.ravel(), math.pi * np.arange(9) / 4, rtol=0, atol=1e-15)
+
+
+def engine_with_state(n=16, species=({"n": 300, "density_ratio": 843.0}, {"n": 120, "density_ratio": 100.0}),
+                      seed=0, steps=2):
+    cfg = make_config(n, species=list(species), Re=80.0, itrmax=6)
+    e = OracleEngine(cfg)
+    rng = np.random.default_rng(seed)
+    nx = cfg.dims[0]
+    e.upload_flow(*[rng.standard_normal((nx, nx, nx)) * 0.3 for _ in range(3)], np.zeros((nx, nx, nx)))
+    for s in range(int(cfg.n_species)):
+        m = int(cfg.species[s].nvalid)
+        pos = [rng.random(m) * 2 * math.pi for _ in range(3)]
+        e.upload_particles(s, np.full(m, 0.01), *pos, *[np.zeros(m)] * 3, ids=np.arange(1, m + 1) + 1000 * s)
+        e.init_particle_velocity(s)
+    e.step(steps)
+    return cfg, e
+
+
+def test_restart_round_trip_and_layout(tmp_path):
+    lib = load_oracle()
+    cfg, a = engine_with_state()
+    path = str(tmp_path / "restart.h5.2")
+    restart.save(a, path)
+    assert restart.listing(lib, path) == ["flow", "particles"]
+    assert restart.listing(lib, path, "flow") == ["P", "U", "V", "W"]
+    assert restart.listing(lib, path, "particles") == ["1", "2"]
+    assert restart.listing(lib, path, "particles/1") == ["counts", "diam", "id", "u", "v", "w", "x", "y", "z"]
+    U = restart.dataset(lib, path, "flow/U")
+    assert U.shape == (16, 16, 16) and U.dtype == np.float64
+    assert np.array_equal(U, a.download_flow()[0])
+    assert restart.dataset(lib, path, "particles/2/counts").tolist() == [120]
+    assert np.array_equal(restart.dataset(lib, path, "particles/2/id"), a.download_particles(1)["ids"])
+    b = OracleEngine(cfg)
+    restart.load(b, path)
+    for x, y in zip(a.download_flow(), b.download_flow()):
+        assert np.array_equal(x, y)
+    for s in range(2):
+        pa, pb = a.download_particles(s), b.download_particles(s)
+        for k in ("ids", "diam", "x", "y", "z", "u", "v", "w"):
+            assert np.array_equal(pa[k], pb[k]), (s, k)
+    a.close()
+    b.close()
+
+
+def test_writer_encodings_match_libhdf5(tmp_path):
+    """The F64 datatype message, the symbol node and the local heap's
+    end-of-free-list value as libhdf5 writes them (read from the SciPy file)."""
+    ref = open(libhdf5_file(), "rb").read()
+    base = 512
+    lib = load_oracle()
+    cfg = make_config(8, mode=_abi.MODE_FLOW)
+    eng = OracleEngine(cfg)
+    eng.upload_flow(*[np.zeros((8, 8, 8))] * 4)
+    path = str(tmp_path / "r.h5")
+    restart.save(eng, path)
+    ours = open(path, "rb").read()
+    eng.close()
+    f64 = bytes.fromhex("11203f000800000000004000340b0034ff030000")
+    assert f64 in ref and f64 in ours
+    # superblock: version 0, 8-byte offsets/lengths, K = 4 / 16
+    assert ours[:8] == ref[base:base + 8] and ours[8:16] == bytes([0, 0, 0, 0, 0, 8, 8, 0])
+    assert struct.unpack("<HH", ours[16:20]) == struct.unpack("<HH", ref[base + 16:base + 20]) == (4, 16)
+    # every local heap ends its free list with offset 1, as libhdf5 does
+    for src, off in ((ours, 0), (ref, base)):
+        i = src.find(b"HEAP")
+        assert i >= 0 and src[i + 4] == 0
+        free = struct.unpack("<Q", src[i + 16:i + 24])[0]
+        assert free == 1 or free < struct.unpack("<Q", src[i + 8:i + 16])[0]
+    assert ours.count(b"SNOD") >= 2 and ours[ours.find(b"SNOD") + 4] == 1
+    assert restart.listing(lib, path, "/") == ["flow"]
+
+
+def test_restart_load_coarse_upsamples(tmp_path):
+    lib = load_oracle()
+    coarse_cfg = make_config(16, mode=_abi.MODE_FLOW)
+    c = OracleEngine(coarse_cfg)
+    rng = np.random.default_rng(3)
+    fields = [rng.standard_normal((16, 16, 16)) for _ in range(4)]
+    c.upload_flow(*fields)
+    path = str(tmp_path / "coarse.h5")
+    restart.save(c, path)
+    fine_cfg = make_config(32, mode=_abi.MODE_FLOW)
+    a, b = OracleEngine(fine_cfg), OracleEngine(fine_cfg)
+    restart.load_coarse(a, path)
+    b.upload_flow_coarse(*fields)
+    for x, y in zip(a.download_flow(), b.download_flow()):
+        assert np.array_equal(x, y)
+    for e in (a, b, c):
+        e.close()
+
+
+def test_stat_state_and_errors(tmp_path):
+    lib = load_oracle()
+    path = str(tmp_path / "stat.h5")
+    restart.save_state(lib, path, 1200, 3.25, 0.0025)
+    assert restart.load_state(lib, path, 1200) == (3.25, 0.0025)
+    assert restart.dataset(lib, path, "1200/state/step").tolist() == 1200
+    with pytest.raises(Exception):
+        restart.load_state(lib, path, 7)
+    cfg, a = engine_with_state(steps=0)
+    rpath = str(tmp_path / "r.h5")
+    restart.save(a, rpath)
+    other = OracleEngine(make_config(24, species=[{"n": 300, "density_ratio": 843.0}]))
+    with pytest.raises(Exception) as exc:
+        restart.load(other, rpath)
+    assert getattr(exc.value, "code", None) == _abi.EINVAL
+    fewer = OracleEngine(make_config(16, species=[{"n": 299, "density_ratio": 843.0}]))
+    with pytest.raises(Exception) as exc:
+        restart.load(fewer, rpath)
+    assert "counts" in str(exc.value)
+    with pytest.raises(Exception):
+        restart.load(a, str(tmp_path / "missing.h5"))
+    open(str(tmp_path / "junk.h5"), "wb").write(b"not hdf5" * 100)
+    with pytest.raises(Exception):
+        restart.load(a, str(tmp_path / "junk.h5"))
+    for e in (a, other, fewer):
+        e.close()

@@ -1792,7 +1792,7 @@ class Engine : public EngineBase {
     const double rmax = pc->search_cell_size * hmin;
     out->nbins = nbins;
     lcs_logrange(pc->min_radius, rmax, nbins + 1, out->edges);
-    const size_t need = std::max<size_t>((size_t)(nbins + 1) * 16, 0);
+    const size_t need = (size_t)(nbins + 1) * 16;  // edges, then the counters
     const int nshells = spectrum_shells(pc->max_wavenumber);
     const int npairs = nshells * ns;
     const unsigned int nbx = 148 * 2;

@@ -305,6 +305,10 @@ int lcs_batch_step(lcs_batch* b, int32_t nsteps, lcs_log* logs) {
       if (rc != LCS_OK) {
         first_rc = rc;
         first_err = "batch group " + std::to_string(gi) + ": " + handle_error(nullptr);
+        for (int32_t q : b->group_members[gi]) {  // members whose steps were enqueued before the failure
+          int32_t d = 0;
+          if (lcs_step_poll(b->members[q], &d) == LCS_OK) begun[q] = 1;
+        }
       } else {
         for (int32_t q : b->group_members[gi]) begun[q] = 1;
       }

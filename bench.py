@@ -317,6 +317,14 @@ def run_b200(args):
     traffic = (SWEEP_DRAM_BYTES_PER_CELL_FP32 if T == 4 else SWEEP_DRAM_BYTES_PER_CELL).get(sweep_kernel)
     traffic = traffic * n3 if traffic else None
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in sorted(tot.items(), key=lambda kv: -kv[1][0])}
+    # HBM-roofline fraction of every kernel with a byte model (algorithmic
+    # bytes per launch; the profiled steps' CUDA-event averages)
+    n_ = int(rc.dims[0])
+    for k, alg in kernel_bytes(n_, int(rc.abi.halo_size), T, np_tot / max(1, len(rc.species))).items():
+        if k in kernels and kernels[k]["launches"]:
+            ms_l = kernels[k]["ms"] / kernels[k]["launches"]
+            gbs = alg / (ms_l / 1e3) / 1e9
+            kernels[k].update({"alg_bytes_per_launch": alg, "gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 3)})
 
     # end to end through the public API: pinned host state in, the per-step
     # timestep!/evolve! calls of the Julia shim, state out
@@ -609,6 +617,26 @@ def run_serve(args):
 
 
 # ------------------------------------------------------------ particle cell index
+def kernel_bytes(n, h, T, particles_per_launch):
+    """Algorithmic DRAM bytes per launch of the step's kernels (n^3 grid, halo
+    h, T-byte field elements):
+    - hsmac_rw: U, V, W, P read and written once per cell, 8T x n^3;
+    - hsmac_faces: the same per cell of the six face slabs of the first
+      time-blocked sweep's box -1..n+3 around the core 2..n;
+    - synchalo: the couple's fill (radius h, all 26 directions, U, V, W): one
+      read and one write per halo cell;
+    - rhs_update: stage 1 reads U, V, W, P, writes U2, V2, W2 (7T); stage 2
+      also reads U2, V2, W2 (10T): the mean, 8.5T x n^3;
+    - particles: 13 FP64 properties read or written a particle, the mean of the
+      two stages (104 and 152 B), the fluid gathers being cache traffic;
+    - cfl_max: U, V, W read once (3T x n^3)."""
+    n3 = float(n) ** 3
+    slab = float(n + 5) ** 3 - float(n - 1) ** 3
+    halo = float(n + 2 * h) ** 3 - n3
+    return {"hsmac_rw": 8 * T * n3, "hsmac_faces": 8 * T * slab, "synchalo": 3 * 2 * T * halo,
+            "rhs_update": 8.5 * T * n3, "particles": 128.0 * particles_per_launch, "cfl_max": 3 * T * n3}
+
+
 def makeindex_bytes(n, H):
     """Algorithmic DRAM bytes of one makeindex of n particles over H cells, as
     this design moves them: positions 24 + keys/indices 8 (cell_hash); the

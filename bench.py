@@ -71,6 +71,12 @@ SWEEP_DRAM_BYTES_PER_CELL = {"hsmac_rw": 69.6}
 # the FP32 form: 588.8 MB and 629.6 MB per launch (profiles/hsmac_rw_fp32_rc256.md)
 SWEEP_DRAM_BYTES_PER_CELL_FP32 = {"hsmac_rw": 36.3}
 SWEEP_KERNELS = ("hsmac_rw", "hsmac_tma", "hsmac_fused")
+# FP64 operations per interior cell of one rhs!+update! launch (k_rhs, both
+# stages alike): smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on
+# of `ncu ... -k regex:k_rhs -c 2` on the lp128 workload (profiles/rhs_lp128.md):
+# 484.4 M adds + 471.9 M multiplies, no FMA (the library is built without
+# contraction), over 128^3 cells.
+RHS_FLOPS_PER_CELL = 456.0
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
@@ -317,6 +323,19 @@ def run_b200(args):
     traffic = (SWEEP_DRAM_BYTES_PER_CELL_FP32 if T == 4 else SWEEP_DRAM_BYTES_PER_CELL).get(sweep_kernel)
     traffic = traffic * n3 if traffic else None
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in sorted(tot.items(), key=lambda kv: -kv[1][0])}
+    # FP64 roofline of rhs! + update!: the measured FMA peak of this GPU
+    import ctypes as C
+
+    fp64_peak = C.c_double()
+    fp64 = None
+    if args.precision == "fp64" and eng.lib.lcs_measure_fp64_peak(rc.abi.device, C.byref(fp64_peak)) == 0 \
+            and "rhs_update" in tot:
+        ms_r, cnt_r = tot["rhs_update"]
+        tf = RHS_FLOPS_PER_CELL * n3 / (ms_r / cnt_r / 1e3) / 1e12
+        fp64 = {"peak_tflops": round(fp64_peak.value, 2), "peak_kind": "measured (k_fp64_peak, FMA chains)",
+                "rhs_flops_per_cell": RHS_FLOPS_PER_CELL, "rhs_tflops": round(tf, 2),
+                "rhs_frac": round(tf / fp64_peak.value, 3),
+                "note": "rhs has no FMA (no contraction): add/multiply issue at half the FMA rate"}
     # HBM-roofline fraction of every kernel with a byte model (algorithmic
     # bytes per launch; the profiled steps' CUDA-event averages)
     n_ = int(rc.dims[0])
@@ -400,6 +419,7 @@ def run_b200(args):
                          "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum",
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
             "kernels": kernels,
+            "fp64": fp64,
             "e2e": {"value": e2e_value, "unit": "Mcell-steps/s",
                     "h2d_bytes_per_step": (h2d1 - h2d0) / e2e_steps, "d2h_bytes_per_step": (d2h1 - d2h0) / e2e_steps,
                     "steps": e2e_steps, "path": "upload + per-step lcs_timestep/lcs_evolve + download"},

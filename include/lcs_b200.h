@@ -151,6 +151,10 @@ LCS_API const char* lcs_last_error(const lcs_handle* h);
 LCS_API int lcs_get_config(const lcs_handle* h, lcs_config* out);
 /* Bytes of device memory the handle holds (the serving admission uses it). */
 LCS_API int lcs_footprint(const lcs_config* cfg, int64_t* bytes);
+/* The device's FP64 FMA throughput in TFLOP/s, measured with a kernel of
+ * independent fused multiply-add chains (the denominator of the FP64
+ * roofline of compute-heavy kernels such as rhs!). */
+LCS_API int lcs_measure_fp64_peak(int32_t device, double* tflops);
 
 /* ---- state transfer (host FP64 in every precision form) ---------------- */
 /* Interior U,V,W,P in, halos left for the next synchalo (src/flows/inits/init.jl). */

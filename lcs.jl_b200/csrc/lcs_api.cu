@@ -81,7 +81,61 @@ static int validate(const lcs_config* c, std::string* why) {
   return LCS_OK;
 }
 
+// FP64 FMA throughput: every thread runs 8 independent chains of fused
+// multiply-adds (values stay bounded); the sums are stored so nothing is
+// dropped.  2 flops per FMA.
+__global__ void __launch_bounds__(512) k_fp64_peak(double* out, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) x[q] = 1e-3 * (threadIdx.x + q);
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) x[q] = __fma_rn(x[q], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) s += x[q];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 extern "C" {
+
+int lcs_measure_fp64_peak(int32_t device, double* tflops) {
+  if (!tflops) return set_global_error(LCS_EINVAL, "null output");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return set_global_error(LCS_EINVAL, "no such CUDA device");
+  }
+  cudaSetDevice(device);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const int blocks = sms * 4, threads = 512, iters = 4096;
+  double* out = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaMalloc(&out, (size_t)blocks * threads * sizeof(double));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int rep = 0; rep < 6 && e == cudaSuccess; rep++) {  // the first launch warms up
+    cudaEventRecord(e0, st);
+    k_fp64_peak<<<blocks, threads, 0, st>>>(out, iters, 0.9999999, 1e-7);
+    cudaEventRecord(e1, st);
+    e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    float ms = 0.f;
+    if (e == cudaSuccess && rep > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) best = ms < best ? ms : best;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) cudaStreamDestroy(st);
+  cudaFree(out);
+  if (e != cudaSuccess) return set_global_error(LCS_ECUDA, cudaGetErrorString(e));
+  *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (best * 1e-3) / 1e12;
+  return LCS_OK;
+}
 
 int lcs_footprint(const lcs_config* cfg, int64_t* bytes) {
   std::string why;

@@ -914,6 +914,12 @@ void lcs_destroy(lcs_handle* h) {
 
 const char* lcs_last_error(const lcs_handle* h) { return h ? h->err : g_err; }
 
+int lcs_measure_fp64_peak(int32_t device, double* tflops) {
+  (void)device;
+  (void)tflops;
+  return fail(NULL, LCS_EINVAL, "the CPU oracle has no device");
+}
+
 int lcs_get_config(const lcs_handle* h, lcs_config* out) {
   if (!h || !out) return LCS_EINVAL;
   *out = h->cfg;

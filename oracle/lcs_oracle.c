@@ -1317,6 +1317,15 @@ int lcs_flow_forcing(lcs_handle* h, double dtrk, double* p, double* e10) {
  * (makeindex.jl:54-58: sortperm! then sortbyperm! of hashes and every
  * property), then the binary searches of src/utils/fast.jl:8-40 for starts and
  * stops of every hash 1..(nc+2)^3 (makeindex.jl:60-66). */
+/* Utils.encode / sub2ind over axes of lengths len[] starting at 0 (hasher.jl:15-38) */
+static int64_t encode_cell(const int64_t len[3], const int ci[3]) {
+  int64_t hash = 1, stride = 1;
+  for (int a = 0; a < 3; a++) {
+    hash += (int64_t)ci[a] * stride; /* offset from the axis start 0 */
+    stride *= len[a];
+  }
+  return hash;
+}
 typedef struct { int64_t h, i; } hash_idx;
 static int cmp_hash_idx(const void* a, const void* b) {
   const hash_idx *x = (const hash_idx*)a, *y = (const hash_idx*)b;
@@ -1370,13 +1379,10 @@ int lcs_particles_makeindex(lcs_handle* h, int32_t s, int32_t stage, int32_t rat
   sp->ci_stops = (int64_t*)malloc((size_t)H * sizeof(int64_t));
   sp->ci_H = H;
   for (int64_t i = 0; i < n; i++) {
-    int64_t hash = 1, stride = 1;
-    for (int a = 0; a < 3; a++) {
-      int ci = (int)floor((sp->p[pos + a][i] - DOMAIN_ORIGIN) / dxc[a]) + 1;
-      hash += (int64_t)ci * stride; /* offset from the axis start 0 */
-      stride *= nc[a] + 2;
-    }
-    hi[i].h = hash;
+    int ci[3];
+    const int64_t len[3] = {nc[0] + 2, nc[1] + 2, nc[2] + 2};
+    for (int a = 0; a < 3; a++) ci[a] = (int)floor((sp->p[pos + a][i] - DOMAIN_ORIGIN) / dxc[a]) + 1;
+    hi[i].h = encode_cell(len, ci);
     hi[i].i = i;
   }
   qsort(hi, (size_t)n, sizeof *hi, cmp_hash_idx);
@@ -1616,6 +1622,21 @@ int lcs_synchronize(lcs_handle* h) { return h ? LCS_OK : LCS_EINVAL; }
 
 /* ---- oracle-only helpers for the known-answer tests -------------------- */
 int lcs_oracle_kcount(int k0) { return kcount(k0); }
+/* test hooks of the cell index: the binary searches and the hasher */
+void lcs_oracle_searchsorted(const int64_t* v, int64_t n, int64_t x, int64_t* first, int64_t* last) {
+  *first = sorted_first(v, n, x);
+  *last = sorted_last(v, n, x);
+}
+int64_t lcs_oracle_cell_encode(const int64_t len[3], const int32_t ci[3]) {
+  const int c[3] = {ci[0], ci[1], ci[2]};
+  return encode_cell(len, c);
+}
+void lcs_oracle_cell_decode(const int64_t len[3], int64_t hash, int32_t ci[3]) {
+  const int nc[3] = {(int)len[0] - 2, (int)len[1] - 2, (int)len[2] - 2};
+  int c[3];
+  decode_cell(hash, nc, c);
+  for (int a = 0; a < 3; a++) ci[a] = c[a];
+}
 int lcs_oracle_kset(int k0, int32_t* out, int cap) {
   int tmp[256][3];
   int n = kset(k0, tmp, cap < 256 ? cap : 256);

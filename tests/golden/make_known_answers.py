@@ -107,6 +107,27 @@ def main(ref):
     no, _ = find_line(lines, r"indices_with_halo_periodic = ")
     out["halo_periodic"] = {"expect": "after synchalo!(FullHalo(h)) A == A_g[mod1.(i, n)...] on the haloed box",
                             "source": f"lib/topologies/test/test_mpi.jl:{no}"}
+    tu = os.path.join(ref, "test/test_utils.jl")
+    lines = open(tu).read().splitlines()
+    no, _ = find_line(lines, r'@testset "searchedsort2"')
+    samples = []
+    for k, ln in enumerate(lines[no:no + 20], no + 1):
+        m = re.match(r"\s*\(\[([0-9, ]*)\], (-?\d+)\),", ln)
+        if m:
+            v = [int(x) for x in m.group(1).split(",") if x.strip()]
+            samples.append({"v": v, "x": int(m.group(2)), "source": f"test/test_utils.jl:{k}"})
+    out["searchsorted"] = {"samples": samples,
+                           "expect": "Utils.searchsortedfirst/last (src/utils/fast.jl:8-40) equal Base's"}
+    sub = []
+    for k, ln in enumerate(lines, 1):
+        m = re.search(r"Utils\.sub2ind\(ranges, \((\d+), (\d+)\)\) == (\d+)", ln)
+        if m:
+            sub.append({"ranges": [[1, 3], [1, 4]], "sub": [int(m.group(1)), int(m.group(2))], "ind": int(m.group(3)),
+                        "source": f"test/test_utils.jl:{k}"})
+    no, _ = find_line(lines, r"hasher = Utils\.Hasher\(\(0:5, 0:5, 0:5\)\)")
+    out["hasher"] = {"sub2ind": sub, "roundtrip_axes": [[0, 5], [0, 5], [0, 5]],
+                     "expect": "encode(x) == LinearIndices((6,6,6))[x .+ 1] and decode(encode(x)) == x",
+                     "source": f"test/test_utils.jl:{no}"}
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)

@@ -232,3 +232,50 @@ def test_particle_periodic_wrap_invariant():  # test/test_particles_mpi.jl:46-61
         shift = np.where(x < 0, L, np.where(x >= L, -L, 0.0))
         assert np.array_equal(X, x + shift)
         assert np.array_equal(e.prop_get(0, _abi.PROP_X2), partner + shift)
+
+
+def test_searchsorted_samples():  # test/test_utils.jl:78-94
+    """The binary searches of src/utils/fast.jl:8-40 (the oracle's starts and
+    stops) on the reference's samples, against Base's definitions
+    (searchsortedfirst = bisect_left + 1, searchsortedlast = bisect_right)."""
+    import bisect
+    import ctypes as C
+
+    lib = load_oracle()
+    f = lib.lcs_oracle_searchsorted
+    f.restype = None
+    f.argtypes = [C.POINTER(C.c_int64), C.c_int64, C.c_int64, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    samples = KA["searchsorted"]["samples"]
+    assert len(samples) == 11
+    for smp in samples:
+        v, x = smp["v"], smp["x"]
+        arr = (C.c_int64 * max(1, len(v)))(*v)
+        a, b = C.c_int64(), C.c_int64()
+        f(arr, len(v), x, C.byref(a), C.byref(b))
+        assert (a.value, b.value) == (bisect.bisect_left(v, x) + 1, bisect.bisect_right(v, x)), smp
+
+
+def test_hasher_known_answers_and_round_trip():  # test/test_utils.jl:103-127
+    """sub2ind on ranges (1:3, 1:4) and the encode/decode round trip over
+    0:5 x 0:5 x 0:5 (LinearIndices), through the oracle's cell hash."""
+    import ctypes as C
+
+    lib = load_oracle()
+    enc, dec = lib.lcs_oracle_cell_encode, lib.lcs_oracle_cell_decode
+    enc.restype, enc.argtypes = C.c_int64, [C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+    dec.restype, dec.argtypes = None, [C.POINTER(C.c_int64), C.c_int64, C.POINTER(C.c_int32)]
+    for k in KA["hasher"]["sub2ind"]:  # axes starting at 1: offsets sub - 1
+        (l0, h0), (l1, h1) = k["ranges"]
+        ln = (C.c_int64 * 3)(h0 - l0 + 1, h1 - l1 + 1, 1)
+        ci = (C.c_int32 * 3)(k["sub"][0] - l0, k["sub"][1] - l1, 0)
+        assert enc(ln, ci) == k["ind"], k
+    ln = (C.c_int64 * 3)(6, 6, 6)
+    lin = np.arange(1, 217).reshape((6, 6, 6), order="F")  # LinearIndices((6, 6, 6))
+    out = (C.c_int32 * 3)()
+    for i in range(6):
+        for j in range(6):
+            for kk in range(6):
+                h = enc(ln, (C.c_int32 * 3)(i, j, kk))
+                assert h == lin[i, j, kk]
+                dec(ln, h, out)
+                assert tuple(out) == (i, j, kk)

@@ -1667,7 +1667,7 @@ class Engine : public EngineBase {
       cg.dxc[a] = (kDomainLength / g.n[a]) * ratio;  // LCS.spacings(grid) .* grid_ratio
       H *= cg.nc[a] + 2;
     }
-    if (H > (int64_t)UINT32_MAX || n > (int64_t)UINT32_MAX) return fail(LCS_EINVAL, "cell index too large");
+    if (H >= (int64_t)INT32_MAX || n > (int64_t)INT32_MAX) return fail(LCS_EINVAL, "cell index too large");  // 32-bit sort and scan sizes
     if (c.ratio != ratio) {  // (re)allocate for this cell size
       LCS_CUDA(cudaStreamSynchronize(stream));
       free_index(c);

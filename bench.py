@@ -297,6 +297,7 @@ def run_b200(args):
     with ClockSampler(rc.abi.device) as clk:
         logs, ms = eng.step_timed(args.steps)
     barrier(world)
+    div_rms, div_max = eng.flow_divergence()  # of the state after the timed steps
     ms_max = reduce_max(ms, world)
     value = world * n3 * args.steps / (ms_max / 1e3) / 1e6
     pvalue = world * np_tot * args.steps / (ms_max / 1e3)
@@ -420,6 +421,8 @@ def run_b200(args):
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
             "kernels": kernels,
             "fp64": fp64,
+            "divergence": {"rms": div_rms, "max": div_max, "last_couple_residual": logs[-1]["couple2"]["div"],
+                           "note": "of the velocity after the timed steps, HSMAC form, interior cells"},
             "e2e": {"value": e2e_value, "unit": "Mcell-steps/s",
                     "h2d_bytes_per_step": (h2d1 - h2d0) / e2e_steps, "d2h_bytes_per_step": (d2h1 - d2h0) / e2e_steps,
                     "steps": e2e_steps, "path": "upload + per-step lcs_timestep/lcs_evolve + download"},

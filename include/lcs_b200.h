@@ -246,6 +246,11 @@ typedef struct lcs_flow_stats {
   double k, epsilon, tau_eta, l_mu, l_eta, Re_lambda, urms, k_eta, skewness, flatness, L, C_epsilon;
 } lcs_flow_stats;
 LCS_API int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* out);
+/* Divergence of the current velocity over the n^3 interior cells, in the
+ * HSMAC form (hsmac.jl: dxi (U[i]-U[i-1]) + dyi (V[j]-V[j-1]) + dzi
+ * (W[k]-W[k-1]), periodic): its RMS and its max |div| (a diagnostic beside the
+ * couple log's residual, which the reference takes over 1:n+1). */
+LCS_API int lcs_flow_divergence(lcs_handle* h, double* rms, double* maxabs);
 
 /* `Particles.makeindex!` (src/particles/makeindex.jl:29-67) on species s with
  * the positions of stage (1: xss, 2: xss2): cell index ci = floor(x / dxc) + 1

@@ -263,6 +263,10 @@ void lcs_group_destroy(lcs_group* gr) {
   delete gr->g;
   delete gr;
 }
+int lcs_flow_divergence(lcs_handle* h, double* rms, double* maxabs) {
+  H(h);
+  return h->e->flow_divergence(rms, maxabs);
+}
 int lcs_upload_flow_coarse(lcs_handle* h, const double* U, const double* V, const double* W, const double* P) {
   H(h);
   return h->e->upload_flow_coarse(U, V, W, P);

@@ -1623,6 +1623,23 @@ class Engine : public EngineBase {
     o.C_epsilon = 0.0;
     return LCS_OK;
   }
+  // divergence of the current velocity (diagnostic): RMS and max over n^3
+  int flow_divergence(double* rms, double* maxabs) override {
+    LCS_TRY(check_flow());
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    const int64_t total = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const unsigned int nb = blocks_for(total, 256, 148 * 8);
+    LCS_TRY(launch("div_stat", k_div_stat<T>, dim3(nb), dim3(256), 0, (const Ctx*)dctx, g, hc.dxi, hc.dyi, hc.dzi,
+                   partials));
+    LCS_TRY(launch("div_stat_final", k_div_stat_final, dim3(1), dim3(256), 0, (const double*)partials, (int)nb, stage));
+    double v[2];
+    LCS_TRY(copy(v, stage, sizeof v, cudaMemcpyDeviceToHost));
+    LCS_TRY(collect_profile());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    if (rms) *rms = std::sqrt(v[0] / (double)total);
+    if (maxabs) *maxabs = v[1];
+    return LCS_OK;
+  }
   static void free_index(CellIndex& c) {
     cudaFree(c.hashes);
     cudaFree(c.starts);

@@ -938,6 +938,52 @@ __global__ void __launch_bounds__(256) k_flow_stat(const Ctx* __restrict__ ctx, 
 }
 
 // Combine the block values in a fixed order (1 block); result in out[0..13].
+// Divergence of the velocity over the interior cells, in the HSMAC form
+// (hsmac.jl: dxi (U[i] - U[i-1]) + dyi (V[j] - V[j-1]) + dzi (W[k] - W[k-1]),
+// periodic reads): per block the sum of div^2 and the max |div|.
+template <typename T>
+__global__ void __launch_bounds__(256) k_div_stat(const Ctx* __restrict__ ctx, Grid g, double dxi, double dyi,
+                                                  double dzi, double* __restrict__ partials) {
+  __shared__ double sh[8];
+  const T* U = (const T*)ctx->vel[kSetUs][0];
+  const T* V = (const T*)ctx->vel[kSetUs][1];
+  const T* W = (const T*)ctx->vel[kSetUs][2];
+  const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+  const int64_t total = (int64_t)nx * ny * nz;
+  double s2 = 0.0, mx = 0.0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % nx), j = 1 + (int)((t / nx) % ny), k = 1 + (int)(t / ((int64_t)nx * ny));
+    const int64_t c = g.at(i, j, k);
+    const double dudx = dxi * (-(double)U[g.at(wrap1(i - 1, nx), j, k)] + (double)U[c]);
+    const double dvdy = dyi * (-(double)V[g.at(i, wrap1(j - 1, ny), k)] + (double)V[c]);
+    const double dwdz = dzi * (-(double)W[g.at(i, j, wrap1(k - 1, nz))] + (double)W[c]);
+    const double div = dudx + dvdy + dwdz;
+    s2 += div * div;
+    mx = fmax(mx, fabs(div));
+  }
+  const double bs = block_sum<256>(s2, sh);
+  const double bm = block_max<256>(mx, sh);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = bs;
+    partials[2 * blockIdx.x + 1] = bm;
+  }
+}
+__global__ void __launch_bounds__(256) k_div_stat_final(const double* __restrict__ partials, int nb,
+                                                        double* __restrict__ out) {
+  __shared__ double sh[8];
+  double s = 0.0, m = 0.0;
+  for (int b = threadIdx.x; b < nb; b += 256) {
+    s += partials[2 * b];
+    m = fmax(m, partials[2 * b + 1]);
+  }
+  const double bs = block_sum<256>(s, sh);
+  const double bm = block_max<256>(m, sh);
+  if (threadIdx.x == 0) {
+    out[0] = bs;
+    out[1] = bm;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_flow_stat_final(const double* __restrict__ partials, int nb,
                                                          double* __restrict__ out) {
   __shared__ double sh[8];

@@ -212,6 +212,12 @@ class Engine:
         self._check(self.lib.lcs_particles_density(self.handle, species, grid_ratio, _dptr(out)))
         return out
 
+    def flow_divergence(self):
+        """(RMS, max |div|) of the current velocity over the interior cells."""
+        r, m = C.c_double(), C.c_double()
+        self._check(self.lib.lcs_flow_divergence(self.handle, C.byref(r), C.byref(m)))
+        return r.value, m.value
+
     def flow_stat(self) -> dict:
         """`Flows.stat` (src/flows/stat.jl:66-153) computed on the device."""
         st = _abi.FlowStat()

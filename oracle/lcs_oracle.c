@@ -914,6 +914,28 @@ void lcs_destroy(lcs_handle* h) {
 
 const char* lcs_last_error(const lcs_handle* h) { return h ? h->err : g_err; }
 
+static int wrapi(int i, int n);
+int lcs_flow_divergence(lcs_handle* h, double* rms, double* maxabs) {
+  if (!h) return LCS_EINVAL;
+  const grid_t* g = &h->g;
+  const int nx = g->n[0], ny = g->n[1], nz = g->n[2];
+  const double dxi = 1.0 / spacing(g, 0), dyi = 1.0 / spacing(g, 1), dzi = 1.0 / spacing(g, 2);
+  double s2 = 0.0, mx = 0.0;
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        const double dudx = dxi * (-h->U[IX(g, wrapi(i - 1, nx), j, k)] + h->U[IX(g, i, j, k)]);
+        const double dvdy = dyi * (-h->V[IX(g, i, wrapi(j - 1, ny), k)] + h->V[IX(g, i, j, k)]);
+        const double dwdz = dzi * (-h->W[IX(g, i, j, wrapi(k - 1, nz))] + h->W[IX(g, i, j, k)]);
+        const double div = dudx + dvdy + dwdz;
+        s2 += div * div;
+        mx = fmax(mx, fabs(div));
+      }
+  if (rms) *rms = sqrt(s2 / ((double)nx * ny * nz));
+  if (maxabs) *maxabs = mx;
+  return LCS_OK;
+}
+
 int lcs_measure_fp64_peak(int32_t device, double* tflops) {
   (void)device;
   (void)tflops;

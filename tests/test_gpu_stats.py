@@ -43,3 +43,24 @@ def test_device_flow_stat_fp32_form():
     got, ref = e.flow_stat(), stats.flow_stat(Uf, Vf, Wf, nu)
     for k in KEYS:
         assert math.isclose(got[k], ref[k], rel_tol=1e-12), (k, got[k], ref[k])
+
+
+@pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_FP32_MIXED])
+def test_device_divergence_equals_oracle(precision):
+    n = 48
+    cfg = make_config(n, mode=_abi.MODE_FLOW)
+    g = Engine(make_config(n, mode=_abi.MODE_FLOW, precision=precision))
+    o = OracleEngine(cfg)
+    U, V, W, P = inits.spectral_flow(n, seed=9)
+    rng = np.random.default_rng(3)
+    U = U + 1e-3 * rng.standard_normal(U.shape)  # not divergence-free
+    g.upload_flow(U, V, W, P)
+    o.upload_flow(*g.download_flow())  # the values the device holds (FP32-rounded in that form)
+    (ra, ma), (rb, mb) = g.flow_divergence(), o.flow_divergence()
+    assert math.isclose(ra, rb, rel_tol=1e-12), (ra, rb)
+    if precision == _abi.PRECISION_FP64:
+        assert ma == mb
+    else:  # the FP32 form's object code may fuse the FP64 multiply-adds
+        assert math.isclose(ma, mb, rel_tol=1e-12)
+    g.close()
+    o.close()

@@ -68,3 +68,26 @@ def test_oracle_flow_stat_equals_host_restatement():
         assert got[c + "_max"] == float(a.max()) and got[c + "_min"] == float(a.min())
     assert got["L"] == 0.0 and got["C_epsilon"] == 0.0
     e.close()
+
+
+def test_oracle_divergence_of_known_fields():
+    """lcs_flow_divergence on the oracle: zero for fields independent of their
+    own axis, and the restated HSMAC difference for a cosine (periodic)."""
+    from helpers import make_config
+    from lcs_b200 import _abi
+    from oracle_engine import OracleEngine
+
+    n = 16
+    e = OracleEngine(make_config(n, mode=_abi.MODE_FLOW))
+    z, y, x = np.meshgrid(*[np.arange(1, n + 1)] * 3, indexing="ij")
+    e.upload_flow(np.sin(y * 0.3), np.cos(z * 0.7), np.sin(x * 1.1), np.zeros((n, n, n)))
+    rms, mx = e.flow_divergence()
+    assert rms == 0.0 and mx == 0.0
+    U = np.cos(2 * np.pi * x / n)
+    e.upload_flow(U, np.zeros_like(U), np.zeros_like(U), np.zeros_like(U))
+    dxi = n / (2 * np.pi)
+    div = dxi * (-np.roll(U, 1, axis=2) + U)
+    rms, mx = e.flow_divergence()
+    assert math.isclose(rms, math.sqrt(np.mean(div ** 2)), rel_tol=1e-13)
+    assert mx == np.abs(div).max()
+    e.close()

@@ -698,6 +698,20 @@ def run_makeindex(args):
         t = eng.profile_totals()
         return t["makeindex"][0], {k: v[0] for k, v in t.items()}
 
+    def push_ms(reps=3):
+        """Device ms of one motion! pass (the fluid gathers) over every species."""
+        for s in range(nsp):
+            eng.particles_motion(s, 1)
+        eng.profile(True)
+        eng.profile_reset()
+        for _ in range(reps):
+            for s in range(nsp):
+                eng.particles_motion(s, 1)
+        t = eng.profile_totals()["particles"][0] / reps
+        eng.profile(False)
+        return t
+
+    push_random_ms = push_ms()  # upload order: uniform random positions
     index_all()  # buffers allocated; the random order is restored below
     eng.synchronize()
     reps = max(1, min(args.steps, 3))
@@ -725,6 +739,7 @@ def run_makeindex(args):
     steady_ms, parts_ms = device_ms()
     steady_ms /= args.steps
     eng.profile(False)
+    push_sorted_ms = push_ms()  # the order makeindex! left
     hashes, starts, stops = eng.particles_cellindex(0, ratio)
     ok = bool(np.all(np.diff(hashes) >= 0)) and int(np.sum(stops - starts + 1)) == hashes.size
     # Particles.stat of every species with the reference's production settings
@@ -758,6 +773,10 @@ def run_makeindex(args):
         "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
                      "peak_source": peak_src, "algorithmic_bytes": algo},
         "invariants_ok": ok, "gpu_launches_total": launches,
+        "particle_push": {"random_order_ms": push_random_ms, "cell_order_ms": push_sorted_ms,
+                          "speedup": push_random_ms / push_sorted_ms,
+                          "note": "motion! of all species (interpolation gathers of U, V, W), device ms, on the "
+                                  "upload order and on the cell order makeindex! leaves"},
         "particle_stat": {"wall_ms": stat_wall_ms, "device_ms": stat_ms,
                           "note": "Particles.stat of all 3 species (Summary, makeindex!, rdf, spectrum 19 shells x "
                                   "64 directions)"},

@@ -756,6 +756,25 @@ def run_makeindex(args):
     stat_wall_ms = (time.perf_counter() - t0) * 1e3
     stat_ms = {k: v[0] for k, v in eng.profile_totals().items()}
     eng.profile(False)
+
+    # the particle kernels (boundary!, motion!, update!, both stages) of one
+    # whole step: on the upload order, then with lcs_set_particle_sort(1)
+    def step_particles_ms():
+        eng.profile(True)
+        eng.profile_reset()
+        eng.step(1)
+        t = eng.profile_totals()["particles"][0]
+        eng.profile(False)
+        return t
+
+    for s, (d, x, y, z) in enumerate(parts):
+        zero = np.zeros_like(x)
+        eng.upload_particles(s, d, x, y, z, zero, zero, zero)
+    step_random_ms = step_particles_ms()
+    eng.set_particle_sort(1, ratio)
+    eng.step(1)  # followed by the first sort
+    step_sorted_ms = step_particles_ms()
+    eng.set_particle_sort(0, ratio)
     launches = eng.launch_count()
     eng.close()
     peak, peak_src = hbm_peak()
@@ -775,8 +794,11 @@ def run_makeindex(args):
         "invariants_ok": ok, "gpu_launches_total": launches,
         "particle_push": {"random_order_ms": push_random_ms, "cell_order_ms": push_sorted_ms,
                           "speedup": push_random_ms / push_sorted_ms,
+                          "step_random_order_ms": step_random_ms, "step_sorted_every_step_ms": step_sorted_ms,
                           "note": "motion! of all species (interpolation gathers of U, V, W), device ms, on the "
-                                  "upload order and on the cell order makeindex! leaves"},
+                                  "upload order and on the cell order makeindex! leaves; step_*: the particle kernels "
+                                  "of one whole step (both stages), on the upload order and with "
+                                  "lcs_set_particle_sort(1, 4)"},
         "particle_stat": {"wall_ms": stat_wall_ms, "device_ms": stat_ms,
                           "note": "Particles.stat of all 3 species (Summary, makeindex!, rdf, spectrum 19 shells x "
                                   "64 directions)"},

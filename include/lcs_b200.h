@@ -260,6 +260,17 @@ LCS_API int lcs_flow_divergence(lcs_handle* h, double* rms, double* maxabs);
  * every property (the device order of the species changes; ids follow), and
  * starts/stops of every hash 1..(nc+2)^3 (src/utils/fast.jl:8-40). */
 LCS_API int lcs_particles_makeindex(lcs_handle* h, int32_t species, int32_t stage, int32_t grid_ratio);
+/* Keep the particles in cell order (no reference counterpart): after every
+ * step of lcs_step or lcs_step_begin that brings the step counter to a
+ * multiple of `interval`, makeindex! (as lcs_particles_makeindex, stage 1,
+ * this grid_ratio) runs on every species.  The fluid gathers of motion! then
+ * read neighbouring cells together.  Each particle's arithmetic does not depend
+ * on its place in the arrays, so a particle's values (matched by id) are those
+ * of the unsorted run, bit for bit; only the order changes.  interval = 0
+ * turns it off (the default).  lcs_evolve does not sort: a caller stepping
+ * with lcs_timestep/lcs_evolve calls lcs_particles_makeindex itself.  Steps of
+ * a batch group (lcs_group_step_begin) refuse members that sort (ESTATE). */
+LCS_API int lcs_set_particle_sort(lcs_handle* h, int32_t interval, int32_t grid_ratio);
 /* The last cell index of species s: hashes[nvalid], starts[(nc+2)^3],
  * stops[(nc+2)^3] (Int64, as LCS.IP); NULL pointers are skipped. */
 LCS_API int lcs_particles_cellindex(lcs_handle* h, int32_t species, int64_t* hashes, int64_t* starts, int64_t* stops);

@@ -138,6 +138,9 @@ end
 
 makeindex!(h, s, stage, grid_ratio) =
     check(h, ccall((:lcs_particles_makeindex, LIB), Cint, (Ptr{Cvoid}, Int32, Int32, Int32), h, s, stage, grid_ratio))
+# keep particles in cell order: makeindex! after every `interval`-th lcs_step step
+set_particle_sort!(h, interval, grid_ratio) =
+    check(h, ccall((:lcs_set_particle_sort, LIB), Cint, (Ptr{Cvoid}, Int32, Int32), h, interval, grid_ratio))
 function particle_stat(h, s, pc::LcsParticleStatConfig, tau_eta::Float64)
     out = Ref{LcsParticleStats}()
     check(h, ccall((:lcs_particles_stat, LIB), Cint,

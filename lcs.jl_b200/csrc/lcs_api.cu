@@ -221,6 +221,10 @@ int lcs_step_poll(lcs_handle* h, int32_t* done) {
 }
 int lcs_step_finish(lcs_handle* h, lcs_log* logs) { H(h); return h->e->step_finish(logs); }
 int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* out) { H(h); return h->e->flow_stat(out); }
+int lcs_set_particle_sort(lcs_handle* h, int32_t interval, int32_t ratio) {
+  H(h);
+  return h->e->set_particle_sort(interval, ratio);
+}
 int lcs_particles_makeindex(lcs_handle* h, int32_t s, int32_t stage, int32_t ratio) {
   H(h);
   return h->e->particles_makeindex(s, stage, ratio);

@@ -55,6 +55,7 @@ struct EngineBase {
   virtual int set_tuning(int rw_rows, int zchunk, double share) = 0;
   virtual int flow_stat(lcs_flow_stats* out) = 0;
   virtual int particles_makeindex(int s, int stage, int grid_ratio) = 0;
+  virtual int set_particle_sort(int interval, int grid_ratio) = 0;
   virtual int particles_cellindex(int s, int64_t* hashes, int64_t* starts, int64_t* stops) = 0;
   virtual int particles_stat(int s, const lcs_particle_stat_config* pc, double tau_eta, lcs_particle_stats* out) = 0;
   virtual int particles_density(int s, int grid_ratio, double* densities) = 0;

@@ -1407,6 +1407,7 @@ class Engine : public EngineBase {
     for (int q = 0; q < nsteps; q++) {
       LCS_CUDA(cudaGraphLaunch(step_exec, stream));
       launches += graph_launches_per_step;
+      LCS_TRY(sort_after(host_step + q + 1));
     }
     return async_tail(nsteps);
   }
@@ -1483,6 +1484,7 @@ class Engine : public EngineBase {
   int step_body(int nsteps, lcs_log* logs, cudaEvent_t e0, cudaEvent_t e1) {
     const bool graphs = cfg.use_graphs && !prof;
     if (graphs) LCS_TRY(build_step_graph());
+    if (sort_interval > 0 && !host_step_known) LCS_TRY(read_ctx());
     if (e0) LCS_CUDA(cudaEventRecord(e0, stream));
     if (!graphs) {
       for (int q = 0; q < nsteps; q++) {
@@ -1495,6 +1497,7 @@ class Engine : public EngineBase {
         if (hctx->wait_error) return fail(LCS_ETIMEDOUT, "a bounded device wait (TMA tile load or grid barrier) ran out");
         if (hctx->nonfinite) return fail(LCS_ENONFINITE, "non-finite residual or dt at step %lld", (long long)hctx->step);
         if (logs) fill_log(hctx->cur, &logs[q]);
+        LCS_TRY(sort_after(hctx->step));
       }
       if (e1 && nsteps == 0) LCS_CUDA(cudaEventRecord(e1, stream));
       return LCS_OK;
@@ -1506,6 +1509,7 @@ class Engine : public EngineBase {
       for (int q = 0; q < chunk; q++) {
         LCS_CUDA(cudaGraphLaunch(step_exec, stream));
         launches += graph_launches_per_step;
+        LCS_TRY(sort_after(host_step + q + 1));  // host_step: the counter before this chunk
       }
       if (e1 && done + chunk == nsteps) LCS_CUDA(cudaEventRecord(e1, stream));
       LCS_TRY(read_ctx());
@@ -1673,6 +1677,15 @@ class Engine : public EngineBase {
     LCS_TRY(check_species(s));
     LCS_TRY(check_stage(stage_));
     if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    LCS_TRY(index_alloc(s, ratio));
+    LCS_TRY(makeindex_enqueue(s, stage_));
+    LCS_TRY(collect_profile());
+    LCS_CUDA(cudaStreamSynchronize(stream));
+    return LCS_OK;
+  }
+  // Cell geometry and buffers of species s's index for this grid_ratio
+  // (allocated when the ratio changes: the stream is synchronised first).
+  int index_alloc(int s, int ratio) {
     if (ratio < 1 || g.n[0] % ratio || g.n[1] % ratio || g.n[2] % ratio)
       return fail(LCS_EINVAL, "grid_ratio must be positive and divide the grid dims");
     CellIndex& c = ci[s];
@@ -1708,6 +1721,15 @@ class Engine : public EngineBase {
     }
     c.cg = cg;
     c.H = H;
+    return LCS_OK;
+  }
+  // The index of species s on the stream (after index_alloc): hashes of the
+  // positions of stage_, the stable sort, the permutation of every property,
+  // starts and stops.  Nothing waits for the stream.
+  int makeindex_enqueue(int s, int stage_) {
+    CellIndex& c = ci[s];
+    const int64_t n = sp[s].n, H = c.H;
+    const CellGeom cg = c.cg;
     cudaEvent_t span = nullptr;  // the whole index, device-timed when profiling
     if (prof && !capturing) {
       span = get_event();
@@ -1746,9 +1768,35 @@ class Engine : public EngineBase {
       cudaEventRecord(b, stream);
       recs.push_back({"makeindex", span, b});
     }
-    LCS_TRY(collect_profile());
-    LCS_CUDA(cudaStreamSynchronize(stream));
     c.built = true;
+    return LCS_OK;
+  }
+
+  // Particle sort (no reference counterpart): every sort_interval-th step of
+  // lcs_step / lcs_step_begin is followed by makeindex! of every species on
+  // its positions, so that the fluid gathers of the next steps read
+  // neighbouring cells together.  Each particle's arithmetic does not depend
+  // on its place in the arrays, so only the order changes (ids follow).
+  int sort_interval = 0, sort_ratio = 0;
+  int set_particle_sort(int interval, int ratio) override {
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    if (interval < 0) return fail(LCS_EINVAL, "interval < 0");
+    if (interval > 0) {
+      if (cfg.mode != LCS_MODE_FLOW_PARTICLE || cfg.n_species < 1)
+        return fail(LCS_EINVAL, "the particle sort needs the flow-particle mode");
+      for (int s = 0; s < cfg.n_species; s++) LCS_TRY(index_alloc(s, ratio));  // buffers before any step
+    }
+    sort_interval = interval;
+    sort_ratio = ratio;
+    return LCS_OK;
+  }
+  // after the step that brought the step counter to `step`
+  int sort_after(int64_t step) {
+    if (sort_interval <= 0 || step % sort_interval != 0) return LCS_OK;
+    for (int s = 0; s < cfg.n_species; s++) {
+      LCS_TRY(index_alloc(s, sort_ratio));  // a no-op unless a stat changed the ratio
+      LCS_TRY(makeindex_enqueue(s, 1));
+    }
     return LCS_OK;
   }
   int particles_cellindex(int s, int64_t* hashes, int64_t* starts, int64_t* stops) override {
@@ -2119,6 +2167,8 @@ struct EngineGroup : GroupBase {
       if (m->rw_variant != mem[0]->rw_variant || m->zchunk_force != mem[0]->zchunk_force ||
           m->sm_share != mem[0]->sm_share)
         return fail(LCS_EINVAL, "group members differ in launch shapes");
+    for (auto* m : mem)
+      if (m->sort_interval > 0) return fail(LCS_ESTATE, "a group step does not sort particles: a member has a particle sort");
     for (size_t q = 0; q < mem.size(); q++)
       if (gens[q] != mem[q]->tuning_gen) drop();
     if (!exec) LCS_TRY(build());

@@ -243,6 +243,7 @@ PROTOTYPES = {
                                             C.c_double, _P, _P]),
     "lcs_flow_stat": (C.c_int, [_P, C.POINTER(FlowStat)]),
     "lcs_particles_makeindex": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
+    "lcs_set_particle_sort": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "lcs_particles_cellindex": (C.c_int, [_P, C.c_int32, _I64, _I64, _I64]),
     "lcs_particles_stat": (C.c_int, [_P, C.c_int32, C.POINTER(ParticleStatConfig), C.c_double,
                                      C.POINTER(ParticleStats)]),

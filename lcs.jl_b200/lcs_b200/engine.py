@@ -184,6 +184,11 @@ class Engine:
         """`Particles.makeindex!` (src/particles/makeindex.jl:29-67): sorts the species by cell hash."""
         self._check(self.lib.lcs_particles_makeindex(self.handle, species, stage, grid_ratio))
 
+    def set_particle_sort(self, interval: int, grid_ratio: int = 4):
+        """Keep particles in cell order: makeindex! of every species after every
+        `interval`-th step of `step` (0 turns it off); ids follow the order."""
+        self._check(self.lib.lcs_set_particle_sort(self.handle, interval, grid_ratio))
+
     def particles_cellindex(self, species: int, grid_ratio: int):
         """(hashes, starts, stops) of the last makeindex of the species."""
         nc = [d // grid_ratio for d in self.n]

@@ -68,6 +68,7 @@ struct lcs_handle {
   int64_t step;
   double t;
   int32_t async_n;                 /* steps of a pending lcs_step_begin (run at begin) */
+  int32_t sort_interval, sort_ratio; /* lcs_set_particle_sort */
   int32_t async_rc;
   lcs_log* async_logs;
   char err[512];
@@ -1068,6 +1069,9 @@ int lcs_group_create(lcs_handle* const* members, int32_t m, lcs_group** out) {
 }
 int lcs_group_step_begin(lcs_group* g, int32_t nsteps) {
   if (!g) return fail(NULL, LCS_EINVAL, "null group");
+  for (int32_t q = 0; q < g->m; q++)
+    if (g->h[q]->sort_interval > 0)
+      return fail(NULL, LCS_ESTATE, "a group step does not sort particles: a member has a particle sort");
   for (int32_t q = 0; q < g->m; q++) {
     const int rc = lcs_step_begin(g->h[q], nsteps);
     if (rc) return fail(NULL, rc, "group member %d: %s", q, g->h[q]->err);
@@ -1181,7 +1185,29 @@ int lcs_step(lcs_handle* h, int32_t nsteps, lcs_log* logs) {
     if (rc) return rc;
     rc = evolve(h, dt, logs ? &logs[q] : NULL);
     if (rc) return rc;
+    if (h->sort_interval > 0 && h->step % h->sort_interval == 0)
+      for (int s = 0; s < h->cfg.n_species; s++) {
+        rc = lcs_particles_makeindex(h, s, 1, h->sort_ratio);
+        if (rc) return rc;
+      }
   }
+  return LCS_OK;
+}
+
+/* The particle sort of the CUDA library: makeindex! of every species after
+ * each step of lcs_step that brings the counter to a multiple of interval. */
+int lcs_set_particle_sort(lcs_handle* h, int32_t interval, int32_t ratio) {
+  if (!h) return LCS_EINVAL;
+  if (interval < 0) return fail(h, LCS_EINVAL, "interval < 0");
+  if (interval > 0) {
+    if (h->cfg.mode != LCS_MODE_FLOW_PARTICLE || h->cfg.n_species < 1)
+      return fail(h, LCS_EINVAL, "the particle sort needs the flow-particle mode");
+    const grid_t* g = &h->g;
+    if (ratio < 1 || g->n[0] % ratio || g->n[1] % ratio || g->n[2] % ratio)
+      return fail(h, LCS_EINVAL, "grid_ratio must be positive and divide the grid dims");
+  }
+  h->sort_interval = interval;
+  h->sort_ratio = ratio;
   return LCS_OK;
 }
 

@@ -96,7 +96,7 @@ struct Ctx {
   unsigned int ticket;  // last-block-done counter
   int nonfinite;        // sticky: a NaN/Inf dt or residual was seen
   int wait_error;       // sticky: a bounded device wait (TMA copy, grid barrier) ran out
-  unsigned int gbar_count, gbar_gen;  // grid-wide barrier of cooperative kernels
+  unsigned int gbar_count;  // arrivals at the grid-wide barriers of a cooperative launch (0 between launches)
   double* sp_base[16];  // property block of each species: 16 FP64 properties, then the ids
 };
 

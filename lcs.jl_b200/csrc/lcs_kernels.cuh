@@ -393,23 +393,21 @@ __device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int* p) {
 constexpr long long kGridBarrierCycles = 200000000;  // ~0.1 s at 2 GHz
 constexpr int kGridBarrierPolls = 1 << 24;
 
-__device__ __forceinline__ bool grid_barrier(Ctx* ctx, unsigned int nblocks, int* flag_sh) {
+// Barrier number b (1, 2, ...) of a launch waits until the arrival counter
+// reaches b x nblocks: one fire-and-forget add per block, no reset between
+// barriers.  The block that finishes last resets the counter to 0 for the
+// next launch (every block has then left its last barrier).
+__device__ __forceinline__ bool grid_barrier(Ctx* ctx, unsigned int target, int* flag_sh) {
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned int gen = ld_acquire_gpu(&ctx->gbar_gen);
     __threadfence();  // the block's writes (ordered by the __syncthreads) before the arrival
-    if (atomicAdd(&ctx->gbar_count, 1u) == nblocks - 1) {
-      ctx->gbar_count = 0;
-      __threadfence();
-      atomicAdd(&ctx->gbar_gen, 1u);
-    } else {
-      const long long t0 = clock64();
-      for (int it = 0; ld_acquire_gpu(&ctx->gbar_gen) == gen; it++) {
-        if (it > kGridBarrierPolls || clock64() - t0 > kGridBarrierCycles) {
-          ok = 0;
-          break;
-        }
+    atomicAdd(&ctx->gbar_count, 1u);
+    const long long t0 = clock64();
+    for (int it = 0; ld_acquire_gpu(&ctx->gbar_count) < target; it++) {
+      if (it > kGridBarrierPolls || clock64() - t0 > kGridBarrierCycles) {
+        ok = 0;
+        break;
       }
     }
     __threadfence();
@@ -524,7 +522,7 @@ __device__ __forceinline__ void hsmac_faces_body(Ctx* __restrict__ ctx, const Gr
         if (inr[q]) acc += (double)div * (double)div;
       }
     }
-    if (p < 5 && !grid_barrier(ctx, nb, &flag)) {
+    if (p < 5 && !grid_barrier(ctx, (unsigned int)(p + 1) * nb, &flag)) {
       if (threadIdx.x == 0) ctx->wait_error = 1;
       ok = false;
       break;

@@ -269,7 +269,8 @@ LCS_API int lcs_particles_makeindex(lcs_handle* h, int32_t species, int32_t stag
  * of the unsorted run, bit for bit; only the order changes.  interval = 0
  * turns it off (the default).  lcs_evolve does not sort: a caller stepping
  * with lcs_timestep/lcs_evolve calls lcs_particles_makeindex itself.  Steps of
- * a batch group (lcs_group_step_begin) refuse members that sort (ESTATE). */
+ * a batch group (lcs_group_step_begin) sort each member that has a sort, on
+ * the group's stream between the group's step graphs. */
 LCS_API int lcs_set_particle_sort(lcs_handle* h, int32_t interval, int32_t grid_ratio);
 /* The last cell index of species s: hashes[nvalid], starts[(nc+2)^3],
  * stops[(nc+2)^3] (Int64, as LCS.IP); NULL pointers are skipped. */

@@ -2167,8 +2167,6 @@ struct EngineGroup : GroupBase {
       if (m->rw_variant != mem[0]->rw_variant || m->zchunk_force != mem[0]->zchunk_force ||
           m->sm_share != mem[0]->sm_share)
         return fail(LCS_EINVAL, "group members differ in launch shapes");
-    for (auto* m : mem)
-      if (m->sort_interval > 0) return fail(LCS_ESTATE, "a group step does not sort particles: a member has a particle sort");
     for (size_t q = 0; q < mem.size(); q++)
       if (gens[q] != mem[q]->tuning_gen) drop();
     if (!exec) LCS_TRY(build());
@@ -2178,7 +2176,17 @@ struct EngineGroup : GroupBase {
       LCS_CUDA(cudaEventRecord(ready, mem[q]->stream));
       LCS_CUDA(cudaStreamWaitEvent(s, ready, 0));
     }
-    for (int q = 0; q < nsteps; q++) LCS_CUDA(cudaGraphLaunch(exec, s));
+    for (int q = 0; q < nsteps; q++) {
+      LCS_CUDA(cudaGraphLaunch(exec, s));
+      for (auto* m : mem) {  // a member's particle sort, on the group's stream after the step
+        if (m->sort_interval <= 0) continue;
+        cudaStream_t own = m->stream;
+        m->stream = s;
+        const int rc2 = m->sort_after(m->host_step + q + 1);
+        m->stream = own;
+        if (rc2 != LCS_OK) return member_fail(m, rc2);
+      }
+    }
     for (size_t q = 0; q < mem.size(); q++) {
       Engine<T>* m = mem[q];
       m->launches += per_step[q] * nsteps;

@@ -1069,9 +1069,6 @@ int lcs_group_create(lcs_handle* const* members, int32_t m, lcs_group** out) {
 }
 int lcs_group_step_begin(lcs_group* g, int32_t nsteps) {
   if (!g) return fail(NULL, LCS_EINVAL, "null group");
-  for (int32_t q = 0; q < g->m; q++)
-    if (g->h[q]->sort_interval > 0)
-      return fail(NULL, LCS_ESTATE, "a group step does not sort particles: a member has a particle sort");
   for (int32_t q = 0; q < g->m; q++) {
     const int rc = lcs_step_begin(g->h[q], nsteps);
     if (rc) return fail(NULL, rc, "group member %d: %s", q, g->h[q]->err);

@@ -16,7 +16,7 @@ import numpy as np
 
 from helpers import make_config
 from lcs_b200 import _abi
-from serve_cases import inputs, load_inputs
+from serve_cases import inputs
 
 L = 2 * math.pi
 
@@ -89,23 +89,51 @@ def check_sort_keeps_values(engine_cls, nsteps=4, interval=2, ratio=4, graphs=0,
     return b
 
 
-def check_group_refuses_sorting_member(engine_cls, lib):
-    """A grouped step does not sort: lcs_group_step_begin refuses a member that
-    has a particle sort (ESTATE) and steps nothing."""
+def check_group_sort_equals_alone(engine_cls, lib, nsteps=3):
+    """A batch group (lcs_group_create) whose second member sorts every step:
+    each member's fields and particles (in their order) equal the member
+    stepped alone with the same sort setting, bit for bit."""
     cfg = sort_config()
-    engines = [engine_cls(cfg) for _ in range(2)]
-    for i, e in enumerate(engines):
-        load_inputs(e, cfg, 30 + i)
+    setting = [0, 1]
+
+    def start(i):
+        e = engine_cls(cfg)
+        flow, parts = inputs(cfg, 40 + i)
+        e.upload_flow(*flow)
+        for s, p in enumerate(parts):
+            n = p["x"].size
+            e.upload_particles(s, p["diam"], p["x"], p["y"], p["z"], p["u"], p["v"], p["w"], ids=np.arange(1, n + 1))
+            e.init_particle_velocity(s)
+        if setting[i]:
+            e.set_particle_sort(setting[i], 4)
+        return e
+
+    def state(e):
+        return e.download_flow(), [e.download_particles(s) for s in range(int(cfg.n_species))]
+
+    alone = []
+    for i in range(2):
+        e = start(i)
+        e._check(e.lib.lcs_step_begin(e.handle, nsteps))
+        e._check(e.lib.lcs_step_finish(e.handle, None))
+        alone.append(state(e))
+        e.close()
+    engines = [start(i) for i in range(2)]
     hs = (C.c_void_p * 2)(*[e.handle.value for e in engines])
     grp = C.c_void_p()
     assert lib.lcs_group_create(hs, 2, C.byref(grp)) == 0, lib.lcs_last_error(None)
     try:
-        engines[1].set_particle_sort(1, 4)
-        assert lib.lcs_group_step_begin(grp, 1) == _abi.ESTATE
-        engines[1].set_particle_sort(0, 4)
-        assert lib.lcs_group_step_begin(grp, 1) == 0, lib.lcs_last_error(None)
+        assert lib.lcs_group_step_begin(grp, nsteps) == 0, lib.lcs_last_error(None)
         for e in engines:
             e._check(lib.lcs_step_finish(e.handle, None))
+        for i, e in enumerate(engines):
+            flow, parts = state(e)
+            for a, b in zip(flow, alone[i][0]):
+                assert np.array_equal(a, b), i
+            for s, (pa, pb) in enumerate(zip(parts, alone[i][1])):
+                for k in pa:
+                    assert np.array_equal(pa[k], pb[k]), (i, s, k)
+        assert not np.array_equal(alone[1][1][0]["ids"], np.arange(1, alone[1][1][0]["ids"].size + 1))
     finally:
         lib.lcs_group_destroy(grp)
         for e in engines:

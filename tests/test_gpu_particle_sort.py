@@ -7,7 +7,7 @@ import pytest
 
 from lcs_b200 import Engine, _abi
 from oracle_engine import OracleEngine
-from sort_cases import check_group_refuses_sorting_member, check_sort_keeps_values, run, sort_config
+from sort_cases import check_group_sort_equals_alone, check_sort_keeps_values, run, sort_config
 
 pytestmark = pytest.mark.gpu
 
@@ -37,5 +37,5 @@ def test_sorted_run_equals_oracle(interval):
             assert np.array_equal(pd[k], po[k]), (s, k)
 
 
-def test_group_refuses_sorting_member():
-    check_group_refuses_sorting_member(Engine, Engine._load())
+def test_group_sorts_its_members():
+    check_group_sort_equals_alone(Engine, Engine._load())

@@ -1,5 +1,5 @@
 """The particle sort (lcs_set_particle_sort) on the oracle: values kept per
-particle, cell order after a sort step, argument errors, grouped steps refused."""
+particle, cell order after a sort step, argument errors, grouped steps equal to members alone."""
 
 import pytest
 
@@ -7,7 +7,7 @@ from helpers import make_config
 from lcs_b200 import _abi
 from lcs_b200.engine import LCSError
 from oracle_engine import OracleEngine, load_oracle
-from sort_cases import check_group_refuses_sorting_member, check_sort_keeps_values
+from sort_cases import check_group_sort_equals_alone, check_sort_keeps_values
 
 
 def test_sort_keeps_every_particle_oracle():
@@ -33,5 +33,5 @@ def test_sort_arguments_oracle():
     f.close()
 
 
-def test_group_refuses_sorting_member_oracle():
-    check_group_refuses_sorting_member(OracleEngine, load_oracle())
+def test_group_sorts_its_members_oracle():
+    check_group_sort_equals_alone(OracleEngine, load_oracle())

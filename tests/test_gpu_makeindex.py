@@ -13,7 +13,7 @@ import pytest
 from helpers import make_config
 from lcs_b200 import Engine, _abi
 from oracle_engine import OracleEngine
-from test_makeindex import cell_hash
+from test_makeindex import cell_hash, out_of_domain_positions
 
 pytestmark = pytest.mark.gpu
 L = 2 * math.pi
@@ -176,3 +176,18 @@ def test_makeindex_large_invariants():
     assert np.array_equal(starts, np.searchsorted(hashes, xs, side="left") + 1)
     assert np.array_equal(stops, np.searchsorted(hashes, xs, side="right"))
     g.close()
+
+
+def test_makeindex_outside_the_domain():
+    """Positions just outside [0, 2pi) (halo cells 0 and nc+1): the same hashes,
+    order and properties as the oracle."""
+    n, npart = (32, 32, 32), 20000
+    cfg = make_config(dims=n, species=[{"n": npart, "density_ratio": 843.0}])
+    g, o = Engine(cfg), OracleEngine(cfg)
+    load((g, o), npart, 12, positions=out_of_domain_positions(npart, 12))
+    for ratio in (4, 1):
+        for e in (g, o):
+            e.particles_makeindex(0, 1, ratio)
+        same_index(g, o, ratio)
+    g.close()
+    o.close()

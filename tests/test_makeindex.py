@@ -108,6 +108,30 @@ def test_positions_on_cell_faces_and_many_ties():
     e.close()
 
 
+def out_of_domain_positions(npart, seed):
+    """Positions a step can leave before the next boundary! pass: just below 0,
+    on 0 and 2pi, just below and above 2pi (halo cells 0 and nc+1 of each axis)."""
+    rng = np.random.default_rng(seed)
+    edge = np.array([-1e-12, -0.05, 0.0, np.nextafter(L, 0.0), L, L + 1e-12, L + 0.05, np.nextafter(0.0, -1.0)])
+    out = []
+    for _ in range(3):
+        a = rng.random(npart) * L
+        pick = rng.random(npart) < 0.6
+        a[pick] = rng.choice(edge, int(pick.sum()))
+        out.append(a)
+    return out
+
+
+def test_positions_outside_the_domain():
+    """Hashes in the halo cells 0 and nc+1 (hash axes 0:nc+1, hasher.jl:15-38)."""
+    n, ratio, npart = (16, 16, 16), 4, 600
+    e, before = setup(n, npart, 9, ratio, positions=out_of_domain_positions(npart, 9))
+    hashes, _, _ = check_index(e, before, n, ratio, 1)
+    nc = 16 // ratio
+    assert hashes.min() == 1 and hashes.max() == (nc + 2) ** 3  # both corner halo cells are used
+    e.close()
+
+
 def test_index_errors():
     e, _ = setup((16, 16, 16), 10, 0, 4)
     with pytest.raises(Exception) as exc:

@@ -149,12 +149,15 @@ struct Reader {
         if (hsize > (1u << 26)) return fail("local heap too large");
         std::vector<char> names(hsize + 1, 0);
         if (hsize && !rd(haddr, names.data(), hsize)) return false;
+        btree_nodes = 0;
         return btree(bt, names, out, 0);
       }
     return fail("not a group (no symbol table message)");
   }
+  int btree_nodes = 0;  // nodes visited in one group's B-tree (a malformed tree may loop)
   bool btree(uint64_t at, const std::vector<char>& names, std::map<std::string, uint64_t>* out, int depth) {
     if (depth > 16) return fail("group B-tree too deep");
+    if (++btree_nodes > (1 << 16)) return fail("group B-tree too large");
     unsigned char hd[24];
     if (!rd(at, hd, 24)) return false;
     if (memcmp(hd, "TREE", 4) != 0) return fail("bad B-tree signature");
@@ -233,7 +236,7 @@ struct Reader {
         else if (cls == 0) *kind = 'i';
         else return fail(path + ": datatype class " + std::to_string(cls) + " is not supported");
         have_type = true;
-      } else if (m.type == 0x08 && n >= 2 && (d[0] == 1 || d[0] == 2)) {  // layout, versions 1-2
+      } else if (m.type == 0x08 && n >= 8 && (d[0] == 1 || d[0] == 2)) {  // layout, versions 1-2
         lclass = d[2];
         if (lclass == 1) {
           if (n < 16) return fail("short layout message");

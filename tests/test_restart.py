@@ -153,3 +153,35 @@ def test_stat_state_and_errors(tmp_path):
         restart.load(a, str(tmp_path / "junk.h5"))
     for e in (a, other, fewer):
         e.close()
+
+
+def test_reader_survives_corrupted_files(tmp_path):
+    """Truncated files and files with random bytes overwritten: every read
+    either returns or fails with an error, and never reads outside the file or
+    a message (a crash would end the test run)."""
+    lib = load_oracle()
+    cfg, a = engine_with_state(steps=0)
+    good = str(tmp_path / "good.h5")
+    restart.save(a, good)
+    a.close()
+    blob = open(good, "rb").read()
+    rng = np.random.default_rng(5)
+    bad = str(tmp_path / "bad.h5")
+    cases = [blob[:k] for k in (0, 8, 96, 200, 800, 2000, len(blob) // 2, len(blob) - 1)]
+    for _ in range(150):
+        b = bytearray(blob)
+        head = min(len(b), 4096)  # the superblock, headers, heaps and B-trees sit at the front
+        for at in rng.integers(0, head, int(rng.integers(1, 6))):
+            b[at] = int(rng.integers(0, 256))
+        cases.append(bytes(b))
+    outcomes = {"ok": 0, "error": 0}
+    for c in cases:
+        open(bad, "wb").write(c)
+        for call in (lambda: restart.listing(lib, bad), lambda: restart.dataset(lib, bad, "flow/U"),
+                     lambda: restart.dataset(lib, bad, "particles/1/x")):
+            try:
+                call()
+                outcomes["ok"] += 1
+            except Exception:
+                outcomes["error"] += 1
+    assert outcomes["error"] > 0 and outcomes["ok"] > 0

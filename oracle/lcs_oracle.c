@@ -34,6 +34,13 @@
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
+#else
+#include <time.h>
+static double omp_get_wtime(void) { /* the serial build's wall clock */
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
 #endif
 
 #define DOMAIN_LENGTH (2.0 * 3.14159265358979323846) /* src/LCS.jl:17 */

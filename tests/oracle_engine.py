@@ -11,7 +11,9 @@ from lcs_b200 import _abi
 from lcs_b200.engine import Engine
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-ORACLE_PATH = os.path.join(ROOT, "oracle", "liblcs_oracle.so")
+# LCS_ORACLE_LIBRARY selects another build of the oracle (the sanitizer builds
+# of `make -C oracle asan|tsan`)
+ORACLE_PATH = os.environ.get("LCS_ORACLE_LIBRARY") or os.path.join(ROOT, "oracle", "liblcs_oracle.so")
 
 _lib = None
 

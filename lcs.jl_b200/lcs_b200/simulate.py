@@ -48,11 +48,12 @@ def init_engine(rc: RunConfig, engine_cls=Engine) -> Engine:
     return eng
 
 
-def printstate(step: int, t: float, dt: float, log: dict, out=sys.stdout):
-    """`LCS.printstate` + `printlog` (src/stat.jl:48-85), one line per step."""
+def printstate(step: int, t: float, dt: float, log: dict, out=None):
+    """`LCS.printstate` + `printlog` (src/stat.jl:48-85), one line per step
+    (to `out`, by default the current sys.stdout)."""
     c1, c2 = log["couple1"], log["couple2"]
-    out.write(f"step={step} t={t:.6e} dt={dt:.6e} couple1=(itr={c1['itr']}, div={c1['div']:.3e}) "
-              f"couple2=(itr={c2['itr']}, div={c2['div']:.3e}) p={log['forcing']['p']:.6e}\n")
+    (out or sys.stdout).write(f"step={step} t={t:.6e} dt={dt:.6e} couple1=(itr={c1['itr']}, div={c1['div']:.3e}) "
+                              f"couple2=(itr={c2['itr']}, div={c2['div']:.3e}) p={log['forcing']['p']:.6e}\n")
 
 
 def simulate(config, *, steps: int | None = None, quiet: bool = False, engine_cls=Engine):

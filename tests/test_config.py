@@ -1,0 +1,140 @@
+"""The `.lcs-yaml` reader (LCSIO.readconfig, src/LCSIO/config.jl:6-31, with the
+kind-tagged objects of lib/polyserde/src/PolySerde.jl:35-80) and the
+`LCS.simulate` mirror (src/simulate.jl:13-90), over the CPU oracle."""
+
+import math
+
+import numpy as np
+import pytest
+import yaml
+
+from lcs_b200 import _abi, config as lcfg
+from lcs_b200.simulate import init_engine, simulate
+from oracle_engine import OracleEngine
+
+
+def reference_style(n=16):
+    """A config in the reference's schema (field names of src/config.jl,
+    src/flows/config.jl, src/particles/config.jl), with settings that differ
+    from the workload builder's defaults."""
+    return {
+        "outdir": "output",
+        "mode": {"kind": "flow-particle"},
+        "backend": {"kind": "cuda"},
+        "topo": {"proc_dims": [0, 0, 0], "reorder": False},
+        "grid": {"dims": [n, n, n], "halo_size": 3},
+        "timestep": {"cfl": 0.25, "dtmax": 0.005},
+        "simulate": {"last_step": 4, "interval_stat": 3, "interval_restart": 100},
+        "flow": {
+            "params": {"U0_m_s": 2.0, "L0_m": 0.5, "NU_m2_s": 0.01},
+            "init": {"kind": "spectral", "params": {"seed": 4, "urms": 1.0, "kpeak": 3.0}},
+            "couple": {"kind": "hsmac", "params": {
+                "time_blocking": False, "overlap": True, "coloring": {"kind": "red-black-block", "params": {"size": 2}},
+                "omega": 1.5, "epsp": 1e-6, "itrmin": 4, "itrmax": 9}},
+            "forcing": {"kind": "rc-energy", "params": {"kmin": 1, "kmax": 2, "energy": 0.649, "coarse_size": 4}},
+        },
+        "particles": [
+            {"population": {"valid": 50, "invalid_ratio": 0.0},
+             "params": {"gravity": 0.0, "density_ratio": 843.0}, "drag": {"kind": "nonlinear"},
+             "init": {"position": {"kind": "random", "params": {"seed": 3}}, "velocity": {"kind": "interp"},
+                      "size": {"kind": "const", "params": {"diam_m": 0.01}}}},
+            {"population": {"valid": 30}, "params": {"gravity": 9.8, "density_ratio": 100.0},
+             "init": {"size": {"kind": "const", "params": {"diam_m": 0.002}}}},
+        ],
+    }
+
+
+def test_readconfig_maps_every_field(tmp_path):
+    p = tmp_path / "run.lcs-yaml"
+    p.write_text(yaml.safe_dump(reference_style()))
+    rc = lcfg.readconfig(str(p))
+    c = rc.abi
+    assert rc.dims == (16, 16, 16) and c.halo_size == 3
+    assert (c.cfl, c.dtmax) == (0.25, 0.005)
+    assert (c.U0, c.L0, c.NU) == (2.0, 0.5, 0.01)
+    assert c.mode == _abi.MODE_FLOW_PARTICLE and c.precision == _abi.PRECISION_FP64
+    assert (c.time_blocking, c.overlap) == (0, 1)
+    assert c.coloring == _abi.COLORING_RED_BLACK_BLOCK and c.coloring_block == 2
+    assert (c.omega, c.epsp, c.itrmin, c.itrmax) == (1.5, 1e-6, 4, 9)
+    assert c.forcing == _abi.FORCING_RC_ENERGY
+    assert (c.kmin, c.kmax, c.coarse_size, c.energy) == (1, 2, 4, 0.649)
+    assert c.n_species == 2
+    assert (c.species[0].nvalid, c.species[0].drag, c.species[0].density_ratio) == (50, _abi.DRAG_NONLINEAR, 843.0)
+    assert (c.species[1].nvalid, c.species[1].drag, c.species[1].gravity) == (30, _abi.DRAG_LINEAR, 9.8)
+    # the non-dimensional diameter diam_m / L0 (particles/config.jl:233)
+    assert rc.species[0].diam == 0.01 / 0.5 and rc.species[1].diam == 0.002 / 0.5
+    assert rc.species[0].velocity == "interp" and rc.species[1].velocity == "rest"
+    assert rc.species[0].position_seed == 3
+    assert (rc.last_step, rc.interval_stat) == (4, 3)
+    assert rc.flow_init == "spectral" and rc.flow_init_params["kpeak"] == 3.0
+
+
+def test_workload_builder_round_trips_through_yaml(tmp_path):
+    d = lcfg.workload(32, 0.005, {"kind": "linear-power", "params": {"power": 0.5}}, [0.05, 0.5], [100, 200],
+                      precision="fp32-mixed", itrmax=50, steps=7)
+    p = tmp_path / "w.lcs-yaml"
+    p.write_text(yaml.safe_dump(d))
+    rc = lcfg.readconfig(str(p))
+    c = rc.abi
+    assert c.precision == _abi.PRECISION_FP32_MIXED and c.forcing == _abi.FORCING_LINEAR_POWER and c.power == 0.5
+    assert c.NU == 0.005 and c.itrmax == 50 and rc.last_step == 7
+    assert math.isclose(c.epsp, 1e-8 * 2 * math.pi / 32)
+    Re = 1.0 / 0.005
+    for s, tp in enumerate((0.05, 0.5)):
+        assert math.isclose(lcfg.taup(843.0, Re, rc.species[s].diam), tp, rel_tol=1e-12)
+
+
+@pytest.mark.parametrize("edit,msg", [
+    (lambda d: d["flow"]["couple"].__setitem__("kind", "sor"), "couple kind"),
+    (lambda d: d["grid"].__setitem__("dims", [16, 16]), "3 entries"),
+    (lambda d: d["particles"][0]["init"].__setitem__("size", {"kind": "uniform"}), "size init"),
+    (lambda d: d.__setitem__("backend", {"kind": "tpu"}), "backend kind"),
+    (lambda d: d.__setitem__("particles", d["particles"] * 9), "species"),
+])
+def test_config_errors(edit, msg):
+    d = reference_style()
+    edit(d)
+    with pytest.raises(ValueError) as exc:
+        lcfg.from_dict(d)
+    assert msg in str(exc.value)
+
+
+def small_run(n=16, steps=3, interval=2):
+    d = lcfg.workload(n, 0.01, {"kind": "linear-power", "params": {"power": 0.5}}, [0.1, 0.5], [200, 100],
+                      itrmax=12, steps=steps)
+    d["simulate"]["interval_stat"] = interval
+    return d
+
+
+def test_simulate_equals_a_manual_step_loop():
+    """simulate() = init + `lcs_step` in interval_stat chunks: the same logs and
+    final state as one loop of timestep! + evolve! over the same init."""
+    d = small_run()
+    eng, logs = simulate(d, quiet=True, engine_cls=OracleEngine)
+    assert [lg["step"] for lg in logs] == [1, 2, 3]
+    ref = init_engine(lcfg.from_dict(d), OracleEngine)
+    manual = []
+    for _ in range(3):
+        dt = ref.timestep()
+        manual.append((dt, ref.evolve(dt)))
+    for lg, (dt, ev) in zip(logs, manual):
+        assert lg["dt"] == dt
+        assert lg["couple1"]["itr"] == ev["couple1"]["itr"] and lg["couple2"]["div"] == ev["couple2"]["div"]
+    for a, b in zip(eng.download_flow(), ref.download_flow()):
+        assert np.array_equal(a, b)
+    for s in range(2):
+        pa, pb = eng.download_particles(s), ref.download_particles(s)
+        for k in pa:
+            assert np.array_equal(pa[k], pb[k]), (s, k)
+    # generated ids run on across species (particles/init.jl)
+    ids = np.concatenate([eng.download_particles(s)["ids"] for s in range(2)])
+    assert np.array_equal(np.sort(ids), np.arange(1, 301))
+    eng.close()
+    ref.close()
+
+
+def test_simulate_prints_one_line_per_step(capsys):
+    eng, logs = simulate(small_run(steps=2, interval=5), engine_cls=OracleEngine)
+    out = capsys.readouterr().out.strip().splitlines()
+    assert len(out) == 2 and out[0].startswith("step=1 ") and "couple1=(itr=" in out[0]
+    eng.close()

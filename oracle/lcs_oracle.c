@@ -81,7 +81,7 @@ struct lcs_handle {
   char err[512];
 };
 
-static char g_err[512];
+static _Thread_local char g_err[512]; /* per thread, as in the CUDA library */
 
 static int fail(lcs_handle* h, int code, const char* fmt, ...) {
   va_list ap;

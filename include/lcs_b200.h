@@ -341,6 +341,26 @@ LCS_API int lcs_restart_save(lcs_handle* h, const char* path);
 LCS_API int lcs_restart_load(lcs_handle* h, const char* path);
 LCS_API int lcs_restart_load_coarse(lcs_handle* h, const char* path);
 LCS_API int lcs_stat_state_save(const char* path, int64_t step, double t, double dt);
+/* One `<step>` entry of the stat file as `LCSIO.savestat` (save.jl:1-33)
+ * writes it with Utils.deepwrite (src/utils/hdf5.jl:5-19), the Julia field
+ * names as dataset names (UTF-8), scalars as rank-0 datasets:
+ *   <step>/state/{step,t,dt}, <step>/state/particles/<s+1>/nvalid
+ *   <step>/stat/state/{step,t,dt}
+ *   <step>/stat/flow/{u,v,w}/{mean,max,min}, k, ϵ, τη, lμ, lη, Reλ, urms, kη,
+ *        skew, flat, L, Cϵ                        (FlowStat, flows/stat.jl:22-39)
+ *   <step>/stat/particles/<s+1>/{x,y,z,u,v,w,diam}/{mean,max,min}, τp, St,
+ *        rdf/{gr_contact,npairs_contact,edges,gr,npairs},
+ *        spectrum/{wavenumbers,Enp}               (particles/stat.jl:10-77)
+ *   <step>/log/flow/couple{1,2}/{itr,div}, <step>/log/flow/forcing/{p,e10}
+ * flow, nvalid, particles (n_species entries) and log may be NULL: their
+ * subtrees are left out, as deepwrite writes nothing for `nothing`; empty
+ * arrays and NaN forcing values are left out too.  Like the reference's "cw"
+ * open, the other steps of an existing file are kept and an existing <step>
+ * is replaced (lcs_stat_state_save does the same); the file is rewritten
+ * through a temporary file.  A group holds at most 8192 entries. */
+LCS_API int lcs_stat_save(const char* path, int64_t step, double t, double dt, const lcs_flow_stats* flow,
+                          int32_t n_species, const int64_t* nvalid, const lcs_particle_stats* particles,
+                          const lcs_log* log);
 LCS_API int lcs_stat_state_load(const char* path, int64_t step, double* t, double* dt);
 LCS_API int lcs_h5_dataset(const char* path, const char* name, int32_t* rank, int64_t* dims, char* kind, void* buf,
                            int64_t bytes);

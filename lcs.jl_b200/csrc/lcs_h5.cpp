@@ -25,6 +25,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <cmath>
+#include <deque>
 #include <map>
 #include <memory>
 #include <string>
@@ -208,6 +210,10 @@ struct Reader {
   bool dataset(const std::string& path, std::vector<uint64_t>* dims, char* kind, void* dst, uint64_t dst_bytes) {
     uint64_t oh;
     if (!find(path, &oh)) return false;
+    return dataset_at(oh, path, dims, kind, dst, dst_bytes);
+  }
+  bool dataset_at(uint64_t oh, const std::string& path, std::vector<uint64_t>* dims, char* kind, void* dst,
+                  uint64_t dst_bytes) {
     std::vector<Msg> ms;
     if (!messages(oh, &ms)) return false;
     bool have_space = false, have_type = false, have_layout = false;
@@ -281,6 +287,44 @@ struct Reader {
     if (bytes < dst_bytes) return fail(path + ": short contiguous data");
     return rd(addr, dst, dst_bytes);
   }
+  // Every group and dataset under the group at `oh` (path `prefix`), with the
+  // datasets' data: what a rewrite of the file keeps.
+  struct Item {
+    std::string path;  // "a/b/c"
+    bool group = false;
+    char kind = 'f';
+    std::vector<uint64_t> dims;
+    std::vector<unsigned char> data;
+  };
+  bool walk(uint64_t oh, const std::string& prefix, std::vector<Item>* out, int depth) {
+    if (depth > 32) return fail("groups nested too deeply");
+    std::map<std::string, uint64_t> ch;
+    if (!children(oh, &ch)) return false;
+    for (auto& kv : ch) {
+      Item it;
+      it.path = prefix.empty() ? kv.first : prefix + "/" + kv.first;
+      std::vector<Msg> ms;
+      if (!messages(kv.second, &ms)) return false;
+      bool group = false;
+      for (auto& m : ms) group = group || m.type == 0x11;
+      if (group) {
+        it.group = true;
+        out->push_back(it);
+        if (!walk(kv.second, it.path, out, depth + 1)) return false;
+        continue;
+      }
+      if (!dataset_at(kv.second, it.path, &it.dims, &it.kind, nullptr, 0)) return false;
+      uint64_t count = 1;
+      for (uint64_t v : it.dims) {
+        if (v && count > (1ull << 40) / v) return fail(it.path + ": dataset too large to rewrite");
+        count *= v;
+      }
+      it.data.resize(count * 8);
+      if (!dataset_at(kv.second, it.path, &it.dims, &it.kind, it.data.data(), count * 8)) return false;
+      out->push_back(std::move(it));
+    }
+    return true;
+  }
 };
 
 // ---------------------------------------------------------------- writer
@@ -297,6 +341,7 @@ struct WNode {
   // layout
   uint64_t oh = 0, heap = 0, heap_data = 0, heap_size = 0, btree = 0, data_addr = 0;
   std::vector<uint64_t> snods;
+  std::vector<uint64_t> leaves;    // leaf-level B-tree nodes under a level-1 root (groups of > 256 children)
   std::vector<uint64_t> name_off;  // heap offsets of the sorted children's names
   WNode* child(const std::string& n) {
     for (auto& k : kids)
@@ -344,6 +389,7 @@ struct Writer {
   static constexpr uint64_t kSnodSize = 8 + 2 * kLeafK * 40;
 
   uint64_t at = 96;  // after the superblock
+  bool too_many = false;  // a group beyond 2 kNodeK x 2 kNodeK x 2 kLeafK children
   void sort_kids(WNode& g) {
     std::sort(g.kids.begin(), g.kids.end(), [](const std::unique_ptr<WNode>& a, const std::unique_ptr<WNode>& b) {
       return strcmp(a->name.c_str(), b->name.c_str()) < 0;
@@ -367,6 +413,16 @@ struct Writer {
       n.btree = at;
       at += kBtreeSize;
       const size_t nsn = (n.kids.size() + 2 * kLeafK - 1) / (2 * kLeafK);
+      // one leaf-level node holds 2 kNodeK symbol nodes; above that a level-1
+      // root indexes up to 2 kNodeK leaf nodes
+      const size_t nleaf = (std::max<size_t>(nsn, 1) + 2 * kNodeK - 1) / (2 * kNodeK);
+      if (nleaf > (size_t)(2 * kNodeK)) too_many = true;
+      n.leaves.clear();
+      if (nleaf > 1)
+        for (size_t q = 0; q < nleaf; q++) {
+          n.leaves.push_back(at);
+          at += kBtreeSize;
+        }
       n.snods.clear();
       for (size_t q = 0; q < std::max<size_t>(nsn, 1); q++) {
         n.snods.push_back(at);
@@ -435,22 +491,48 @@ struct Writer {
       b.assign(n.heap_size, 0);
       for (size_t q = 0; q < n.kids.size(); q++) memcpy(&b[n.name_off[q]], n.kids[q]->name.c_str(), n.kids[q]->name.size());
       if (!emit(f, n.heap_data, b)) return false;
-      // B-tree: one leaf level over the symbol nodes; key q+1 = last name in node q
-      b.clear();
-      b.insert(b.end(), {'T', 'R', 'E', 'E'});
-      put(b, 0, 1);
-      put(b, 0, 1);
-      put(b, n.snods.size(), 2);
-      put(b, kUndef, 8);
-      put(b, kUndef, 8);
-      put(b, 0, 8);
-      for (size_t q = 0; q < n.snods.size(); q++) {
-        put(b, n.snods[q], 8);
-        const size_t last = std::min(n.kids.size(), (q + 1) * 2 * kLeafK);
-        put(b, last ? n.name_off[last - 1] : 0, 8);
+      // B-tree over the symbol nodes: key i = the last name in child i-1
+      // (key 0 = the last name before the node's first child, "" at the
+      // start), child i holds the names in (key i, key i+1]
+      const size_t per_leaf = 2 * kNodeK, nsn = n.snods.size();
+      auto last_name = [&](size_t snod_end) -> uint64_t {  // the last name in symbol nodes [0, snod_end)
+        const size_t last = std::min(n.kids.size(), snod_end * 2 * kLeafK);
+        return last ? n.name_off[last - 1] : 0;
+      };
+      auto node = [&](int level, size_t c0, size_t c1, uint64_t left, uint64_t right, uint64_t key0,
+                      const std::vector<uint64_t>& child, const std::vector<uint64_t>& key) {
+        b.clear();
+        b.insert(b.end(), {'T', 'R', 'E', 'E'});
+        put(b, 0, 1);
+        put(b, level, 1);
+        put(b, c1 - c0, 2);
+        put(b, left, 8);
+        put(b, right, 8);
+        put(b, key0, 8);
+        for (size_t q = c0; q < c1; q++) {
+          put(b, child[q], 8);
+          put(b, key[q], 8);
+        }
+        b.resize(kBtreeSize, 0);
+      };
+      std::vector<uint64_t> snod_key(nsn);
+      for (size_t q = 0; q < nsn; q++) snod_key[q] = last_name(q + 1);
+      if (n.leaves.empty()) {
+        node(0, 0, nsn, kUndef, kUndef, 0, n.snods, snod_key);
+        if (!emit(f, n.btree, b)) return false;
+      } else {
+        const size_t nleaf = n.leaves.size();
+        std::vector<uint64_t> leaf_key(nleaf);
+        for (size_t l = 0; l < nleaf; l++) {
+          const size_t s0 = l * per_leaf, s1 = std::min(nsn, s0 + per_leaf);
+          leaf_key[l] = last_name(s1);
+          node(0, s0, s1, l ? n.leaves[l - 1] : kUndef, l + 1 < nleaf ? n.leaves[l + 1] : kUndef,
+               s0 ? last_name(s0) : 0, n.snods, snod_key);
+          if (!emit(f, n.leaves[l], b)) return false;
+        }
+        node(1, 0, nleaf, kUndef, kUndef, 0, n.leaves, leaf_key);
+        if (!emit(f, n.btree, b)) return false;
       }
-      b.resize(kBtreeSize, 0);
-      if (!emit(f, n.btree, b)) return false;
       for (size_t q = 0; q < n.snods.size(); q++) {
         b.clear();
         b.insert(b.end(), {'S', 'N', 'O', 'D'});
@@ -524,7 +606,10 @@ struct Writer {
   }
   int write(const char* path) {
     at = 96;
+    too_many = false;
     layout_meta(root);
+    if (too_many)
+      return io_fail(LCS_EINVAL, "a group holds more than " + std::to_string(8 * kNodeK * kNodeK * kLeafK) + " entries");
     layout_data(root);
     const uint64_t eof = at;
     FILE* f = fopen(path, "wb");
@@ -657,14 +742,160 @@ int lcs_restart_load_coarse(lcs_handle* h, const char* path) {
   return load_flow(h, r, cfg->dims[0] / 2, cfg->dims[1] / 2, cfg->dims[2] / 2, true);
 }
 
+// A save of one step of the stat file.  The reference opens the file "cw" and
+// replaces the step's group (save.jl:17-31); this writer makes whole files, so
+// an existing file is read whole, every entry outside the top-level group
+// `<step>` is kept, and the file is written again under a temporary name that
+// then replaces it.  A file this reader cannot read is left as it is (error).
+struct StatFile {
+  Writer w;
+  std::vector<Reader::Item> kept;
+  std::deque<double> f;  // storage of the new scalars and arrays
+  std::deque<int64_t> i;
+  std::deque<std::vector<double>> fa;
+  std::deque<std::vector<int64_t>> ia;
+  int open(const char* path, const std::string& step) {
+    if (FILE* t = fopen(path, "rb")) {
+      fclose(t);
+      Reader r;
+      if (!r.open(path) || !r.walk(r.root_oh, "", &kept, 0))
+        return io_fail(LCS_EINVAL, std::string(path) + ": " + r.err + " (the file is left unchanged)");
+    }
+    for (auto& it : kept) {
+      if (it.path == step || it.path.compare(0, step.size() + 1, step + "/") == 0) continue;
+      const size_t q = it.path.rfind('/');
+      const std::string g = q == std::string::npos ? "" : it.path.substr(0, q);
+      const std::string name = q == std::string::npos ? it.path : it.path.substr(q + 1);
+      if (it.group)
+        w.group(it.path);
+      else
+        w.dataset(g, name, it.kind, it.dims, it.data.data());
+    }
+    return LCS_OK;
+  }
+  void scalar(const std::string& g, const std::string& name, double v) {
+    f.push_back(v);
+    w.dataset(g, name, 'f', {}, &f.back());
+  }
+  void scalar_i(const std::string& g, const std::string& name, int64_t v) {
+    i.push_back(v);
+    w.dataset(g, name, 'i', {}, &i.back());
+  }
+  void array(const std::string& g, const std::string& name, const double* v, size_t n) {  // empty: not written
+    if (!n) return;
+    fa.emplace_back(v, v + n);
+    w.dataset(g, name, 'f', {(uint64_t)n}, fa.back().data());
+  }
+  void array_i(const std::string& g, const std::string& name, const int64_t* v, size_t n) {
+    if (!n) return;
+    ia.emplace_back(v, v + n);
+    w.dataset(g, name, 'i', {(uint64_t)n}, ia.back().data());
+  }
+  void summary(const std::string& g, const lcs_summary& m) {  // LCS.Summary (src/stat.jl:4-9)
+    scalar(g, "mean", m.mean);
+    scalar(g, "max", m.max);
+    scalar(g, "min", m.min);
+  }
+  int write(const char* path) {
+    const std::string tmp = std::string(path) + ".tmp";
+    const int rc = w.write(tmp.c_str());
+    if (rc != LCS_OK) {
+      remove(tmp.c_str());
+      return rc;
+    }
+    if (rename(tmp.c_str(), path) != 0) {
+      remove(tmp.c_str());
+      return io_fail(LCS_EINVAL, std::string("cannot replace ") + path);
+    }
+    return LCS_OK;
+  }
+};
+
 int lcs_stat_state_save(const char* path, int64_t step, double t, double dt) {
   if (!path) return io_fail(LCS_EINVAL, "null path");
-  Writer w;
-  const std::string g = std::to_string(step) + "/state";
-  w.dataset(g, "step", 'i', {}, &step);
-  w.dataset(g, "t", 'f', {}, &t);
-  w.dataset(g, "dt", 'f', {}, &dt);
-  return w.write(path);
+  const std::string key = std::to_string(step);
+  StatFile sf;
+  if (int rc = sf.open(path, key)) return rc;
+  sf.scalar_i(key + "/state", "step", step);
+  sf.scalar(key + "/state", "t", t);
+  sf.scalar(key + "/state", "dt", dt);
+  return sf.write(path);
+}
+
+// One `<step>` entry of the stat file as LCSIO.savestat writes it
+// (save.jl:1-33): Utils.deepwrite (src/utils/hdf5.jl:5-19) of the normalized
+// State, Stat and log, with the Julia field names as dataset names.
+int lcs_stat_save(const char* path, int64_t step, double t, double dt, const lcs_flow_stats* fs, int32_t ns,
+                  const int64_t* nvalid, const lcs_particle_stats* ps, const lcs_log* lg) {
+  if (!path) return io_fail(LCS_EINVAL, "null path");
+  if (ns < 0 || ns > LCS_MAX_SPECIES) return io_fail(LCS_EINVAL, "species count out of range");
+  for (int32_t s = 0; ps && s < ns; s++)
+    if (ps[s].nbins < 0 || ps[s].nbins > LCS_RDF_MAX_BINS || ps[s].nshells < 0 ||
+        ps[s].nshells > LCS_SPECTRUM_MAX_SHELLS)
+      return io_fail(LCS_EINVAL, "species " + std::to_string(s) + ": bin or shell count out of range");
+  const std::string key = std::to_string(step);
+  StatFile sf;
+  if (int rc = sf.open(path, key)) return rc;
+  // state: LCS.State (src/state.jl:15-22); FlowState has no fields,
+  // ParticleState holds nvalid (src/particles/state.jl:6-8)
+  const std::string st = key + "/state";
+  sf.scalar_i(st, "step", step);
+  sf.scalar(st, "t", t);
+  sf.scalar(st, "dt", dt);
+  for (int32_t s = 0; nvalid && s < ns; s++) sf.scalar_i(st + "/particles/" + std::to_string(s + 1), "nvalid", nvalid[s]);
+  // stat: LCS.Stat (src/stat.jl:26-40) = StateStat, FlowStat, ParticleStat...
+  const std::string ss = key + "/stat";
+  sf.scalar_i(ss + "/state", "step", step);
+  sf.scalar(ss + "/state", "t", t);
+  sf.scalar(ss + "/state", "dt", dt);
+  if (fs) {  // FlowStat (src/flows/stat.jl:22-39)
+    const std::string g = ss + "/flow";
+    sf.summary(g + "/u", lcs_summary{fs->u_mean, fs->u_max, fs->u_min});
+    sf.summary(g + "/v", lcs_summary{fs->v_mean, fs->v_max, fs->v_min});
+    sf.summary(g + "/w", lcs_summary{fs->w_mean, fs->w_max, fs->w_min});
+    sf.scalar(g, "k", fs->k);
+    sf.scalar(g, "\u03F5", fs->epsilon);           // ϵ
+    sf.scalar(g, "\u03C4\u03B7", fs->tau_eta);      // τη
+    sf.scalar(g, "l\u03BC", fs->l_mu);              // lμ
+    sf.scalar(g, "l\u03B7", fs->l_eta);             // lη
+    sf.scalar(g, "Re\u03BB", fs->Re_lambda);        // Reλ
+    sf.scalar(g, "urms", fs->urms);
+    sf.scalar(g, "k\u03B7", fs->k_eta);             // kη
+    sf.scalar(g, "skew", fs->skewness);
+    sf.scalar(g, "flat", fs->flatness);
+    sf.scalar(g, "L", fs->L);
+    sf.scalar(g, "C\u03F5", fs->C_epsilon);         // Cϵ
+  }
+  for (int32_t s = 0; ps && s < ns; s++) {  // ParticleStat, RDFStat, SpectrumStat (src/particles/stat.jl:10-77)
+    const lcs_particle_stats& p = ps[s];
+    const std::string g = ss + "/particles/" + std::to_string(s + 1);
+    sf.summary(g + "/x", p.x);
+    sf.summary(g + "/y", p.y);
+    sf.summary(g + "/z", p.z);
+    sf.summary(g + "/u", p.u);
+    sf.summary(g + "/v", p.v);
+    sf.summary(g + "/w", p.w);
+    sf.summary(g + "/diam", p.diam);
+    sf.scalar(g, "\u03C4p", p.taup);                // τp
+    sf.scalar(g, "St", p.St);
+    sf.scalar(g + "/rdf", "gr_contact", p.gr_contact);
+    sf.scalar_i(g + "/rdf", "npairs_contact", p.npairs_contact);
+    if (p.nbins > 0) sf.array(g + "/rdf", "edges", p.edges, (size_t)p.nbins + 1);
+    sf.array(g + "/rdf", "gr", p.gr, (size_t)p.nbins);
+    sf.array_i(g + "/rdf", "npairs", p.npairs, (size_t)p.nbins);
+    sf.array(g + "/spectrum", "wavenumbers", p.wavenumbers, (size_t)p.nshells);
+    sf.array(g + "/spectrum", "Enp", p.Enp, (size_t)p.nshells);
+  }
+  if (lg) {  // the step's evolve! log (src/evolve.jl:126-145): the couples' (; itr, div), the forcing's (; p[, e10])
+    const std::string g = key + "/log/flow";
+    sf.scalar_i(g + "/couple1", "itr", lg->couple1.itr);
+    sf.scalar(g + "/couple1", "div", lg->couple1.div);
+    sf.scalar_i(g + "/couple2", "itr", lg->couple2.itr);
+    sf.scalar(g + "/couple2", "div", lg->couple2.div);
+    if (!std::isnan(lg->forcing_p)) sf.scalar(g + "/forcing", "p", lg->forcing_p);
+    if (!std::isnan(lg->forcing_e10)) sf.scalar(g + "/forcing", "e10", lg->forcing_e10);
+  }
+  return sf.write(path);
 }
 
 int lcs_stat_state_load(const char* path, int64_t step, double* t, double* dt) {

@@ -259,6 +259,8 @@ PROTOTYPES = {
     "lcs_restart_load": (C.c_int, [_P, C.c_char_p]),
     "lcs_restart_load_coarse": (C.c_int, [_P, C.c_char_p]),
     "lcs_stat_state_save": (C.c_int, [C.c_char_p, C.c_int64, C.c_double, C.c_double]),
+    "lcs_stat_save": (C.c_int, [C.c_char_p, C.c_int64, C.c_double, C.c_double, C.c_void_p, C.c_int32, C.c_void_p,
+                                C.c_void_p, C.c_void_p]),
     "lcs_stat_state_load": (C.c_int, [C.c_char_p, C.c_int64, _D, _D]),
     "lcs_h5_dataset": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int32), _I64, C.c_char_p, C.c_void_p,
                                  C.c_int64]),

@@ -14,6 +14,7 @@ import ctypes as C
 
 import numpy as np
 
+from . import _abi
 from .engine import LCSError
 
 
@@ -36,6 +37,20 @@ def load_coarse(engine, path: str):
 
 def save_state(lib, path: str, step: int, t: float, dt: float):
     _err(lib, lib.lcs_stat_state_save(path.encode(), step, t, dt))
+
+
+def save_stat(lib, path: str, step: int, t: float, dt: float, flow=None, nvalid=None, particles=None, log=None):
+    """`LCSIO.savestat` of one step (lcs_stat_save): `flow` a FlowStat (or its
+    dict), `nvalid` the species' particle counts, `particles` a sequence of
+    ParticleStats, `log` a Log; each may be None."""
+    fs = None
+    if flow is not None:
+        fs = flow if isinstance(flow, _abi.FlowStat) else _abi.FlowStat(**flow)
+    ns = len(particles) if particles is not None else (len(nvalid) if nvalid is not None else 0)
+    nv = (C.c_int64 * max(ns, 1))(*nvalid) if nvalid is not None else None
+    ps = (_abi.ParticleStats * max(ns, 1))(*particles) if particles is not None else None
+    _err(lib, lib.lcs_stat_save(path.encode(), step, t, dt, C.byref(fs) if fs is not None else None, ns,
+                                nv, ps, C.byref(log) if log is not None else None))
 
 
 def load_state(lib, path: str, step: int):

@@ -8,6 +8,7 @@ libhdf5's own layout), whose `testdouble` is pi * [0..8] / 4.  The writer uses
 the same encodings, compared byte for byte where the two overlap.
 """
 
+import ctypes as C
 import math
 import os
 import struct
@@ -185,3 +186,76 @@ def test_reader_survives_corrupted_files(tmp_path):
             except Exception:
                 outcomes["error"] += 1
     assert outcomes["error"] > 0 and outcomes["ok"] > 0
+
+
+FLOW_NAMES = {"u", "v", "w", "k", "ϵ", "τη", "lμ", "lη", "Reλ", "urms", "kη", "skew",
+              "flat", "L", "Cϵ"}
+PARTICLE_NAMES = {"x", "y", "z", "u", "v", "w", "diam", "τp", "St", "rdf", "spectrum"}
+
+
+def test_stat_file_holds_the_reference_tree(tmp_path):
+    """lcs_stat_save: the `<step>` entry of LCSIO.savestat (state, stat, log)
+    with the Julia field names, from the library's own Flows.stat and
+    Particles.stat, and the other steps of the file kept."""
+    lib = load_oracle()
+    cfg, e = engine_with_state(steps=2)
+    log = _abi.Log()
+    e._check(lib.lcs_step(e.handle, 1, C.byref(log)))
+    fs = _abi.FlowStat()
+    e._check(lib.lcs_flow_stat(e.handle, C.byref(fs)))
+    pcfg = _abi.ParticleStatConfig(grid_ratio=4, bin_size=8, search_cell_size=2, max_wavenumber=8, nsamples=16,
+                                   contact_tolerance=0.01, min_radius=1e-3)
+    pstats = []
+    for s in range(2):
+        ps = _abi.ParticleStats()
+        e._check(lib.lcs_particles_stat(e.handle, s, C.byref(pcfg), fs.tau_eta, C.byref(ps)))
+        pstats.append(ps)
+    path = str(tmp_path / "stat.h5")
+    restart.save_state(lib, path, 1, 0.01, 0.01)  # an earlier step, kept by the next save
+    restart.save_stat(lib, path, 3, 0.03, 0.01, flow=fs, nvalid=[300, 120], particles=pstats, log=log)
+    assert restart.listing(lib, path) == ["1", "3"]
+    assert restart.listing(lib, path, "3") == ["log", "stat", "state"]
+    assert set(restart.listing(lib, path, "3/stat")) == {"flow", "particles", "state"}
+    assert set(restart.listing(lib, path, "3/stat/flow")) == FLOW_NAMES
+    assert restart.dataset(lib, path, "3/stat/flow/ϵ").tolist() == fs.epsilon
+    assert restart.dataset(lib, path, "3/stat/flow/Reλ").tolist() == fs.Re_lambda
+    assert restart.dataset(lib, path, "3/stat/flow/u/max").tolist() == fs.u_max
+    assert restart.listing(lib, path, "3/stat/particles") == ["1", "2"]
+    for s, ps in enumerate(pstats):
+        g = f"3/stat/particles/{s + 1}"
+        assert set(restart.listing(lib, path, g)) == PARTICLE_NAMES
+        assert restart.dataset(lib, path, g + "/τp").tolist() == ps.taup
+        assert restart.dataset(lib, path, g + "/diam/mean").tolist() == ps.diam.mean
+        nb, nsh = ps.nbins, ps.nshells
+        assert np.array_equal(restart.dataset(lib, path, g + "/rdf/edges"), np.array(ps.edges[:nb + 1]))
+        assert np.array_equal(restart.dataset(lib, path, g + "/rdf/npairs"), np.array(ps.npairs[:nb]))
+        assert restart.dataset(lib, path, g + "/rdf/npairs_contact").tolist() == ps.npairs_contact
+        assert np.array_equal(restart.dataset(lib, path, g + "/spectrum/Enp"), np.array(ps.Enp[:nsh]))
+        assert restart.dataset(lib, path, f"3/state/particles/{s + 1}/nvalid").tolist() == (300, 120)[s]
+    assert restart.dataset(lib, path, "3/log/flow/couple2/itr").tolist() == log.couple2.itr
+    assert restart.dataset(lib, path, "3/log/flow/couple1/div").tolist() == log.couple1.div
+    assert "forcing" not in restart.listing(lib, path, "3/log/flow")  # no forcing: its log is empty
+    assert restart.load_state(lib, path, 3) == (0.03, 0.01) and restart.load_state(lib, path, 1) == (0.01, 0.01)
+    # saving step 1 again replaces its group and keeps step 3
+    restart.save_state(lib, path, 1, 0.5, 0.25)
+    assert restart.load_state(lib, path, 1) == (0.5, 0.25)
+    assert set(restart.listing(lib, path, "3/stat/flow")) == FLOW_NAMES
+    e.close()
+
+
+def test_stat_file_with_many_steps(tmp_path):
+    """A root group of 600 steps (over 256 entries: a two-level group B-tree),
+    every step read back; a file the reader cannot read is left unchanged."""
+    lib = load_oracle()
+    path = str(tmp_path / "stat.h5")
+    for q in range(600):
+        restart.save_state(lib, path, 10 * q, 0.5 * q, 0.25)
+    names = restart.listing(lib, path)
+    assert sorted(int(x) for x in names) == [10 * q for q in range(600)]
+    for q in range(0, 600, 7):
+        assert restart.load_state(lib, path, 10 * q) == (0.5 * q, 0.25)
+    junk = str(tmp_path / "junk.h5")
+    open(junk, "wb").write(b"x" * 1000)
+    with pytest.raises(Exception):
+        restart.save_state(lib, junk, 1, 0.0, 0.0)
+    assert open(junk, "rb").read() == b"x" * 1000

@@ -161,3 +161,22 @@ restart_save(h, path::AbstractString) = checkio(ccall((:lcs_restart_save, LIB), 
 restart_load!(h, path::AbstractString) = checkio(ccall((:lcs_restart_load, LIB), Cint, (Ptr{Cvoid}, Cstring), h, path))
 restart_load_coarse!(h, path::AbstractString) =
     checkio(ccall((:lcs_restart_load_coarse, LIB), Cint, (Ptr{Cvoid}, Cstring), h, path))
+
+# ---- the stat file (LCSIO.savestat of one step: state, stat and log)
+struct LcsFlowStats
+    u_mean::Float64; u_max::Float64; u_min::Float64
+    v_mean::Float64; v_max::Float64; v_min::Float64
+    w_mean::Float64; w_max::Float64; w_min::Float64
+    k::Float64; epsilon::Float64; tau_eta::Float64; l_mu::Float64; l_eta::Float64; Re_lambda::Float64
+    urms::Float64; k_eta::Float64; skewness::Float64; flatness::Float64; L::Float64; C_epsilon::Float64
+end
+function flow_stat(h)
+    out = Ref{LcsFlowStats}()
+    check(h, ccall((:lcs_flow_stat, LIB), Cint, (Ptr{Cvoid}, Ref{LcsFlowStats}), h, out))
+    out[]
+end
+stat_save(path::AbstractString, step, t, dt, fs::LcsFlowStats, nvalid::Vector{Int64},
+          ps::Vector{LcsParticleStats}, log::LcsLog) =
+    checkio(ccall((:lcs_stat_save, LIB), Cint,
+        (Cstring, Int64, Float64, Float64, Ref{LcsFlowStats}, Int32, Ptr{Int64}, Ptr{LcsParticleStats}, Ref{LcsLog}),
+        path, step, t, dt, fs, length(ps), nvalid, ps, log))

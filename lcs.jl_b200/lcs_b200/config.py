@@ -50,6 +50,11 @@ class SpeciesInit:
     position_seed: int = 0
     velocity: str = "rest"          # "rest" | "interp"
     id_kind: str = "generate"
+    # Cell, RDF and Spectrum of the species' statistics (particles/config.jl:51-108)
+    grid_ratio: int = 4
+    rdf: dict = field(default_factory=lambda: {"contact_tolerance": 0.01, "bin_size": 16, "min_radius": 1.0e-3,
+                                               "search_cell_size": 1})
+    spectrum: dict = field(default_factory=lambda: {"max_wavenumber": 128, "nsamples": 64})
 
 
 @dataclass
@@ -62,6 +67,9 @@ class RunConfig:
     species: list = field(default_factory=list)
     last_step: int = 0
     interval_stat: int = 1
+    interval_restart: int = 0       # 0: no restart files
+    num_restart_files: int = 1
+    outdir: str = "output"
     raw: dict = field(default_factory=dict)
 
     @property
@@ -138,13 +146,19 @@ def from_dict(d: dict) -> RunConfig:
             pk, pp2 = _kind(init.get("position"), "random")
             vk, _ = _kind(init.get("velocity"), "rest")
             idk, _ = _kind(init.get("id"), "generate")
-            species.append(
-                SpeciesInit(nvalid=nvalid, diam=diam, position=pk, position_seed=int(pp2.get("seed", 1000 + s)),
-                            velocity=vk, id_kind=idk)
-            )
+            si = SpeciesInit(nvalid=nvalid, diam=diam, position=pk, position_seed=int(pp2.get("seed", 1000 + s)),
+                             velocity=vk, id_kind=idk)
+            si.grid_ratio = int((pc.get("cell") or {}).get("grid_ratio", si.grid_ratio))
+            st = pc.get("stat") or {}
+            si.rdf.update(st.get("rdf") or {})
+            si.spectrum.update(st.get("spectrum") or {})
+            species.append(si)
     sim = d.get("simulate") or {}
     return RunConfig(abi=c, flow_init=ik, flow_init_params=ip, species=species,
-                     last_step=int(sim.get("last_step", 0)), interval_stat=int(sim.get("interval_stat", 1)), raw=d)
+                     last_step=int(sim.get("last_step", 0)), interval_stat=int(sim.get("interval_stat", 1)),
+                     interval_restart=int(sim.get("interval_restart", 0)),
+                     num_restart_files=int(sim.get("num_restart_files", 1)), outdir=str(d.get("outdir", "output")),
+                     raw=d)
 
 
 def readconfig(path: str) -> RunConfig:

@@ -56,21 +56,76 @@ def printstate(step: int, t: float, dt: float, log: dict, out=None):
                               f"couple2=(itr={c2['itr']}, div={c2['div']:.3e}) p={log['forcing']['p']:.6e}\n")
 
 
-def simulate(config, *, steps: int | None = None, quiet: bool = False, engine_cls=Engine):
-    """Run the configured simulation; returns (engine, logs)."""
+def save_stat(eng, rc: RunConfig, log: dict, path: str):
+    """`LCS.stat` + `LCSIO.savestat` (src/simulate.jl:62-66): Flows.stat and
+    Particles.stat of every species on the device, written as the step's entry
+    of the stat file (the species are reordered by cell, as in the reference)."""
+    import ctypes as C
+
+    from . import restart
+
+    fs = eng.flow_stat()
+    pstats = []
+    for s, si in enumerate(rc.species):
+        pc = _abi.ParticleStatConfig(grid_ratio=si.grid_ratio, bin_size=int(si.rdf["bin_size"]),
+                                     search_cell_size=int(si.rdf["search_cell_size"]),
+                                     max_wavenumber=int(si.spectrum["max_wavenumber"]),
+                                     nsamples=int(si.spectrum["nsamples"]),
+                                     contact_tolerance=float(si.rdf["contact_tolerance"]),
+                                     min_radius=float(si.rdf["min_radius"]))
+        ps = _abi.ParticleStats()
+        eng._check(eng.lib.lcs_particles_stat(eng.handle, s, C.byref(pc), float(fs["tau_eta"]), C.byref(ps)))
+        pstats.append(ps)
+    lg = _abi.Log()
+    for k in ("couple1", "couple2"):
+        getattr(lg, k).itr, getattr(lg, k).sweeps, getattr(lg, k).div = (log[k]["itr"], log[k]["sweeps"],
+                                                                          log[k]["div"])
+    lg.forcing_p, lg.forcing_e10 = log["forcing"]["p"], log["forcing"]["e10"]
+    lg.dt, lg.t, lg.step = log["dt"], log["t"], log["step"]
+    restart.save_stat(eng.lib, path, int(log["step"]), float(log["t"]), float(log["dt"]), flow=fs,
+                      nvalid=[si.nvalid for si in rc.species] or None, particles=pstats or None, log=lg)
+
+
+def simulate(config, *, steps: int | None = None, quiet: bool = False, engine_cls=Engine, save: bool = False,
+             outdir: str | None = None):
+    """Run the configured simulation; returns (engine, logs).
+
+    With save=True, as `LCS.simulate` does through LCSIO: every interval_stat
+    steps the statistics go into `<outdir>/stat.h5` (one group per step), and
+    every interval_restart steps the state into `<outdir>/restart.h5.<step>`,
+    keeping the last num_restart_files of them (LCSIO.cleanrestart)."""
+    import os
+
+    from . import restart
+
     rc = config if isinstance(config, RunConfig) else (readconfig(config) if isinstance(config, str) else from_dict(config))
     eng = init_engine(rc, engine_cls)
     last = rc.last_step if steps is None else steps
-    interval = max(1, rc.interval_stat)
+    istat = max(1, rc.interval_stat)
+    irest = rc.interval_restart if save else 0
+    out = outdir or rc.outdir
+    if save:
+        os.makedirs(out, exist_ok=True)
     logs = []
     done = 0
     while done < last:
-        chunk = min(interval, last - done)
+        # up to the next statistics (or restart) step, device-resident in between
+        chunk = min(istat - done % istat, last - done)
+        if irest > 0:
+            chunk = min(chunk, irest - done % irest)
         for lg in eng.step(chunk):
             logs.append(lg)
             if not quiet:
                 printstate(lg["step"], lg["t"], lg["dt"], lg)
         done += chunk
+        step = int(logs[-1]["step"])
+        if save and step % istat == 0:
+            save_stat(eng, rc, logs[-1], os.path.join(out, "stat.h5"))
+        if irest > 0 and step % irest == 0:
+            restart.save(eng, os.path.join(out, f"restart.h5.{step}"))
+            old = os.path.join(out, f"restart.h5.{step - irest * rc.num_restart_files}")
+            if os.path.isfile(old):
+                os.remove(old)
     return eng, logs
 
 

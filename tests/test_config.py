@@ -3,6 +3,7 @@ kind-tagged objects of lib/polyserde/src/PolySerde.jl:35-80) and the
 `LCS.simulate` mirror (src/simulate.jl:13-90), over the CPU oracle."""
 
 import math
+import os
 
 import numpy as np
 import pytest
@@ -137,4 +138,44 @@ def test_simulate_prints_one_line_per_step(capsys):
     eng, logs = simulate(small_run(steps=2, interval=5), engine_cls=OracleEngine)
     out = capsys.readouterr().out.strip().splitlines()
     assert len(out) == 2 and out[0].startswith("step=1 ") and "couple1=(itr=" in out[0]
+    eng.close()
+
+
+def test_simulate_writes_stat_and_restart_files(tmp_path):
+    """save=True: stat.h5 gets one entry per interval_stat step (the savestat
+    tree), restart.h5.<step> every interval_restart steps with the oldest
+    beyond num_restart_files removed (LCSIO.cleanrestart), and the last restart
+    reloads to the run's final state."""
+    from lcs_b200 import restart
+    from oracle_engine import load_oracle
+
+    d = small_run(steps=6, interval=2)
+    d["simulate"].update({"interval_restart": 3, "num_restart_files": 1})
+    for p in d["particles"]:
+        p["cell"] = {"grid_ratio": 2}
+        p["stat"] = {"rdf": {"contact_tolerance": 0.01, "bin_size": 4, "min_radius": 1e-3, "search_cell_size": 1},
+                     "spectrum": {"max_wavenumber": 6, "nsamples": 8}}
+    rc = lcfg.from_dict(d)
+    assert rc.species[0].grid_ratio == 2 and rc.species[1].spectrum["nsamples"] == 8
+    eng, logs = simulate(rc, quiet=True, engine_cls=OracleEngine, save=True, outdir=str(tmp_path))
+    lib = load_oracle()
+    files = sorted(os.listdir(tmp_path))
+    assert files == ["restart.h5.6", "stat.h5"]
+    stat = str(tmp_path / "stat.h5")
+    assert restart.listing(lib, stat) == ["2", "4", "6"]
+    assert restart.dataset(lib, stat, "4/stat/state/step").tolist() == 4
+    assert restart.dataset(lib, stat, "6/log/flow/couple1/itr").tolist() == logs[5]["couple1"]["itr"]
+    assert restart.dataset(lib, stat, "6/log/flow/forcing/p").tolist() == logs[5]["forcing"]["p"]
+    assert restart.dataset(lib, stat, "6/state/particles/2/nvalid").tolist() == 100
+    k = restart.dataset(lib, stat, "2/stat/particles/1/spectrum/wavenumbers")
+    assert k.size == restart.dataset(lib, stat, "2/stat/particles/1/spectrum/Enp").size and k.max() == 6
+    fresh = OracleEngine(rc.abi)
+    restart.load(fresh, str(tmp_path / "restart.h5.6"))
+    for a, b in zip(fresh.download_flow(), eng.download_flow()):
+        assert np.array_equal(a, b)
+    for s in range(2):
+        pa, pb = fresh.download_particles(s), eng.download_particles(s)
+        for k in pa:
+            assert np.array_equal(pa[k], pb[k]), (s, k)
+    fresh.close()
     eng.close()

@@ -310,6 +310,9 @@ class Engine : public EngineBase {
     constexpr bool f64 = std::is_same<T, double>::value;
     use_tma = c.coloring == LCS_COLORING_RED_BLACK_FAST && sw != "plain";
     use_rw = use_tma && !(f64 && sw == "tma");
+    // the row-warp sweep addresses a field with 32-bit offsets
+    if (use_rw && (uint64_t)g.pz * (uint64_t)(g.n[2] + 2 * g.h) >= (1ull << 32))
+      return fail(LCS_EINVAL, "a field of 2^32 or more elements");
     if (use_tma) LCS_TRY(init_tma());
     LCS_TRY(init_faces());
     LCS_CUDA(cudaStreamSynchronize(stream));

@@ -245,7 +245,10 @@ __device__ __forceinline__ void hsmac_rw_body(Ctx* __restrict__ ctx, const Grid&
       // Planes s_lo .. s_hi need no z masks: every z condition below holds there.
       const int s_lo = max(max(kb + 2, D.lo[2] + 2), max(out.lo[2] + 2, 2));
       const int s_hi = min(min(min(ke + 1, D.hi[2]), min(oz_hi, nz + 1)), out.hi[2] + 1);
-      const int64_t grow = g.at(xL, j, 0);      // HBM offset of the pair at plane 0
+      // HBM offsets in 32 bits (a field holds < 2^32 elements: 13 fields of
+      // 2^32 FP32 values would need 223 GB); a lane whose offset is negative
+      // stores nothing, so its wrapped value is never used
+      const uint32_t grow = (uint32_t)g.at(xL, j, 0), pz32 = (uint32_t)g.pz;
       const int vofs = (w + 1) * W + 2 * lane;  // this row's pair in a velocity plane tile
       const int dofs = w * W + 2 * lane;        // this row's pair in a dp plane
       const int pofs = (w - 1) * W + 2 * lane;  // this row's pair in a P plane tile (rows y0 ..)
@@ -355,7 +358,7 @@ __device__ __forceinline__ void hsmac_rw_body(Ctx* __restrict__ ctx, const Grid&
         // ---- phase Y: U, V, P at s-1 and W at s-2 of the pair
         const T dN = shfl_down1(dm.x);  // dp(xR+1, s-1)
         const T2 pv = Ps2[QM];          // P at s-1
-        const int64_t o1 = grow + (int64_t)k1 * g.pz;
+        const uint32_t o1 = grow + (uint32_t)k1 * pz32;
         if (y1) {
           const T2 dup = lds2(dpm + W);  // final dp of row j+1 at s-1
           const bool mL = z_m && (FULL || (bt.dy && bt.dL)), mR = z_m && (FULL || (bt.dy && bt.dR));
@@ -400,7 +403,7 @@ __device__ __forceinline__ void hsmac_rw_body(Ctx* __restrict__ ctx, const Grid&
           const bool mxL = FULL || (bt.dy && bt.dL), mxR = FULL || (bt.dy && bt.dR);
           const T w0 = face_update_t<T>(wb.x, !R, z_b && mxL, dpb.x, z_m && mxL, dm.x, dzi);
           const T w1 = face_update_t<T>(wb.y, R, z_b && mxR, dpb.y, z_m && mxR, dm.y, dzi);
-          const int64_t o2 = o1 - g.pz;
+          const uint32_t o2 = o1 - pz32;
           if (FULL) {
             if (lane_out) st2<T>(Wo + o2, w0, w1);
           } else {

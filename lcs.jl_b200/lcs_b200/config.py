@@ -48,8 +48,11 @@ class SpeciesInit:
     diam: float                     # non-dimensional diameter diam_m / L0 (particles/config.jl:233)
     position: str = "random"
     position_seed: int = 0
-    velocity: str = "rest"          # "rest" | "interp"
-    id_kind: str = "generate"
+    velocity: str = "rest"          # "rest" | "interp" | "restart"
+    id_kind: str = "generate"       # "generate" | "restart"
+    size: str = "const"             # "const" | "restart"
+    restart_file: str = ""          # ParticleRestart(file, iprofile) of any "restart" kind
+    restart_profile: int = 0
     # Cell, RDF and Spectrum of the species' statistics (particles/config.jl:51-108)
     grid_ratio: int = 4
     rdf: dict = field(default_factory=lambda: {"contact_tolerance": 0.01, "bin_size": 16, "min_radius": 1.0e-3,
@@ -140,14 +143,18 @@ def from_dict(d: dict) -> RunConfig:
             c.species[s].drag = DRAGS[dk]
             init = pc.get("init") or {}
             sk, sp = _kind(init.get("size"), "const")
-            if sk != "const":
+            if sk not in ("const", "restart"):
                 raise ValueError(f"unsupported particle size init {sk!r}")
-            diam = float(sp["diam_m"]) / c.L0
+            diam = float(sp["diam_m"]) / c.L0 if sk == "const" else 0.0
             pk, pp2 = _kind(init.get("position"), "random")
-            vk, _ = _kind(init.get("velocity"), "rest")
-            idk, _ = _kind(init.get("id"), "generate")
+            vk, vp = _kind(init.get("velocity"), "rest")
+            idk, idp = _kind(init.get("id"), "generate")
             si = SpeciesInit(nvalid=nvalid, diam=diam, position=pk, position_seed=int(pp2.get("seed", 1000 + s)),
-                             velocity=vk, id_kind=idk)
+                             velocity=vk, id_kind=idk, size=sk)
+            for k, prm in ((pk, pp2), (vk, vp), (idk, idp), (sk, sp)):  # ParticleRestart (particles/config.jl:150-153)
+                if k == "restart":
+                    si.restart_file = str(prm["file"])
+                    si.restart_profile = int(prm.get("iprofile", s + 1))
             si.grid_ratio = int((pc.get("cell") or {}).get("grid_ratio", si.grid_ratio))
             st = pc.get("stat") or {}
             si.rdf.update(st.get("rdf") or {})

@@ -19,9 +19,18 @@ from .engine import Engine
 
 def init_engine(rc: RunConfig, engine_cls=Engine) -> Engine:
     """`LCS.Buffer` + `LCS.State` + `LCS.init!` (src/init.jl:6-26)."""
+    from . import restart
+
     eng = engine_cls(rc.abi)
     n = rc.dims[0]
-    if rc.flow_init == "spectral":
+    if rc.flow_init in ("restart", "upsample"):  # LCS.Restart / Upsample (flows/inits/init.jl:16-24)
+        f = str(rc.flow_init_params["file"])
+        if rc.flow_init == "restart":
+            U, V, W, P = (restart.dataset(eng.lib, f, "flow/" + c) for c in "UVWP")
+            eng.upload_flow(U, V, W, P)
+        else:
+            restart.load_coarse(eng, f)
+    elif rc.flow_init == "spectral":
         p = rc.flow_init_params
         U, V, W, P = inits.spectral_flow(n, seed=int(p.get("seed", 0)), urms=float(p.get("urms", 1.0)),
                                          kpeak=float(p.get("kpeak", 4.0)))
@@ -29,23 +38,63 @@ def init_engine(rc: RunConfig, engine_cls=Engine) -> Engine:
         U, V, W, P = inits.ideal_flow(n)
     else:
         raise ValueError(f"flow init {rc.flow_init!r} is not available on the B200 backend "
-                         "(random-flow needs Julia's Xoshiro stream; restart/upsample need HDF5)")
-    eng.upload_flow(U, V, W, P)
+                         "(random-flow needs Julia's Xoshiro stream)")
+    if rc.flow_init in ("spectral", "ideal-flow"):
+        eng.upload_flow(U, V, W, P)
     offset = 0
     for s, si in enumerate(rc.species):
-        if si.position != "random":
+        # ParticleRestart (particles/config.jl:150-217): particles/<iprofile>/... of a restart file
+        def from_file(name, si=si):
+            a = restart.dataset(eng.lib, si.restart_file, f"particles/{si.restart_profile}/{name}")
+            if a.size != si.nvalid:
+                raise ValueError(f"{si.restart_file}: particles/{si.restart_profile}/{name} holds {a.size} "
+                                 f"particles, the species {si.nvalid}")
+            return a.reshape(-1)
+        if si.position == "restart":
+            x, y, z = from_file("x"), from_file("y"), from_file("z")
+        elif si.position == "random":
+            x, y, z = inits.random_positions(si.nvalid, si.position_seed)
+        else:
             raise ValueError(f"particle position init {si.position!r} is not available")
-        x, y, z = inits.random_positions(si.nvalid, si.position_seed)
         zeros = np.zeros(si.nvalid)
-        diam = np.full(si.nvalid, si.diam)
-        ids = inits.generate_ids(si.nvalid, offset)
+        u, v, w = (from_file(c) for c in "uvw") if si.velocity == "restart" else (zeros, zeros, zeros)
+        diam = from_file("diam") if si.size == "restart" else np.full(si.nvalid, si.diam)
+        ids = from_file("id") if si.id_kind == "restart" else inits.generate_ids(si.nvalid, offset)
         offset += si.nvalid
-        eng.upload_particles(s, diam, x, y, z, zeros, zeros, zeros, ids=ids)
+        eng.upload_particles(s, diam, x, y, z, u, v, w, ids=ids)
         if si.velocity == "interp":
             eng.init_particle_velocity(s)
-        elif si.velocity != "rest":
+        elif si.velocity not in ("rest", "restart"):
             raise ValueError(f"particle velocity init {si.velocity!r} is not available")
     return eng
+
+
+def latest_restart(outdir: str):
+    """LCSIO.find_latest_restart_file (LCSIO/config.jl:105-120): the
+    restart.h5.<step> of the largest step, and that step; (None, 0) if none."""
+    import os
+    import re
+
+    best, step = None, -1
+    if os.path.isdir(outdir):
+        for f in os.listdir(outdir):
+            m = re.fullmatch(r"restart\.h5\.(\d+)", f)
+            if m and int(m.group(1)) > step:
+                best, step = os.path.join(outdir, f), int(m.group(1))
+    return best, max(step, 0)
+
+
+def patch_resume(rc: RunConfig, file: str) -> RunConfig:
+    """LCSIO.patch_resume (LCSIO/config.jl:80-101): every init reads the restart file."""
+    import copy
+
+    rc = copy.copy(rc)
+    rc.flow_init, rc.flow_init_params = "restart", {"file": file}
+    rc.species = [copy.copy(si) for si in rc.species]
+    for s, si in enumerate(rc.species):
+        si.position = si.velocity = si.id_kind = si.size = "restart"
+        si.restart_file, si.restart_profile = file, s + 1
+    return rc
 
 
 def printstate(step: int, t: float, dt: float, log: dict, out=None):
@@ -87,32 +136,48 @@ def save_stat(eng, rc: RunConfig, log: dict, path: str):
 
 
 def simulate(config, *, steps: int | None = None, quiet: bool = False, engine_cls=Engine, save: bool = False,
-             outdir: str | None = None):
+             outdir: str | None = None, resume: bool | None = None):
     """Run the configured simulation; returns (engine, logs).
 
     With save=True, as `LCS.simulate` does through LCSIO: every interval_stat
     steps the statistics go into `<outdir>/stat.h5` (one group per step), and
     every interval_restart steps the state into `<outdir>/restart.h5.<step>`,
-    keeping the last num_restart_files of them (LCSIO.cleanrestart)."""
+    keeping the last num_restart_files of them (LCSIO.cleanrestart).
+
+    resume (default: the LCS_RESUME environment variable, as LCSIO.init reads
+    it): continue from the latest restart.h5.<step> in outdir, with t from
+    stat.h5 (LCSIO.load_resume_state!), up to step last_step."""
     import os
 
     from . import restart
 
     rc = config if isinstance(config, RunConfig) else (readconfig(config) if isinstance(config, str) else from_dict(config))
+    out = outdir or rc.outdir
+    if resume is None:
+        resume = os.environ.get("LCS_RESUME", "0").lower() in ("1", "true", "yes")
+    start = 0
+    if resume:
+        file, start = latest_restart(out)
+        if file is None:
+            raise ValueError(f"no restart files to resume from in {out}")
+        rc = patch_resume(rc, file)
     eng = init_engine(rc, engine_cls)
-    last = rc.last_step if steps is None else steps
+    if resume:
+        t, _ = restart.load_state(eng.lib, os.path.join(out, "stat.h5"), start)
+        eng.set_state(start, t)
+    last = (rc.last_step - start) if steps is None else steps
     istat = max(1, rc.interval_stat)
     irest = rc.interval_restart if save else 0
-    out = outdir or rc.outdir
     if save:
         os.makedirs(out, exist_ok=True)
     logs = []
     done = 0
     while done < last:
         # up to the next statistics (or restart) step, device-resident in between
-        chunk = min(istat - done % istat, last - done)
+        at = start + done
+        chunk = min(istat - at % istat, last - done)
         if irest > 0:
-            chunk = min(chunk, irest - done % irest)
+            chunk = min(chunk, irest - at % irest)
         for lg in eng.step(chunk):
             logs.append(lg)
             if not quiet:

@@ -179,3 +179,64 @@ def test_simulate_writes_stat_and_restart_files(tmp_path):
             assert np.array_equal(pa[k], pb[k]), (s, k)
     fresh.close()
     eng.close()
+
+
+def test_resume_continues_the_run(tmp_path):
+    """LCS_RESUME: a run stopped at step 3 (restart.h5.3, stat.h5) and resumed
+    to step 6 ends where an uninterrupted 6-step run ends (flow bit for bit,
+    particles by id), with the step counter and time carried over."""
+    d = small_run(steps=3, interval=3)
+    d["simulate"].update({"interval_restart": 3, "num_restart_files": 2})
+    out = str(tmp_path / "run")
+    eng, _ = simulate(d, quiet=True, engine_cls=OracleEngine, save=True, outdir=out)
+    eng.close()
+    d6 = small_run(steps=6, interval=3)
+    d6["simulate"].update({"interval_restart": 3, "num_restart_files": 2})
+    resumed, rlogs = simulate(d6, quiet=True, engine_cls=OracleEngine, save=True, outdir=out, resume=True)
+    assert [lg["step"] for lg in rlogs] == [4, 5, 6]
+    assert sorted(os.listdir(out)) == ["restart.h5.3", "restart.h5.6", "stat.h5"]
+    whole, wlogs = simulate(d6, quiet=True, engine_cls=OracleEngine)
+    assert rlogs[-1]["t"] == wlogs[-1]["t"] and resumed.get_state() == whole.get_state()
+    for a, b in zip(resumed.download_flow(), whole.download_flow()):
+        assert np.array_equal(a, b)
+    for s in range(2):
+        pa, pb = resumed.download_particles(s), whole.download_particles(s)
+        oa, ob = np.argsort(pa["ids"]), np.argsort(pb["ids"])
+        for k in pa:
+            assert np.array_equal(pa[k][oa], pb[k][ob]), (s, k)
+    with pytest.raises(ValueError):
+        simulate(d6, quiet=True, engine_cls=OracleEngine, outdir=str(tmp_path / "empty"), resume=True)
+    resumed.close()
+    whole.close()
+
+
+def test_restart_and_upsample_inits(tmp_path):
+    """flow.init restart / upsample and the particles' restart kinds
+    (ParticleRestart(file, iprofile)) read a restart file through the library."""
+    from lcs_b200 import restart
+
+    d = small_run(steps=2, interval=2)
+    eng, _ = simulate(d, quiet=True, engine_cls=OracleEngine)
+    f = str(tmp_path / "restart.h5.2")
+    restart.save(eng, f)
+    r = small_run()
+    r["flow"]["init"] = {"kind": "restart", "params": {"file": f}}
+    for i, p in enumerate(r["particles"]):
+        rk = {"kind": "restart", "params": {"file": f, "iprofile": i + 1}}
+        p["init"] = {"id": rk, "position": rk, "velocity": rk, "size": rk}
+    again = init_engine(lcfg.from_dict(r), OracleEngine)
+    for a, b in zip(again.download_flow(), eng.download_flow()):
+        assert np.array_equal(a, b)
+    for s in range(2):
+        pa, pb = again.download_particles(s), eng.download_particles(s)
+        for k in pa:
+            assert np.array_equal(pa[k], pb[k]), (s, k)
+    up = small_run(n=32)
+    up["flow"]["init"] = {"kind": "upsample", "params": {"file": f}}
+    fine = init_engine(lcfg.from_dict(up), OracleEngine)
+    ref = OracleEngine(lcfg.from_dict(small_run(n=32)).abi)
+    restart.load_coarse(ref, f)
+    for a, b in zip(fine.download_flow(), ref.download_flow()):
+        assert np.array_equal(a, b)
+    for e in (eng, again, fine, ref):
+        e.close()

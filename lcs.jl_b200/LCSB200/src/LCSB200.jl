@@ -117,13 +117,19 @@ function LCS.evolve!(::LCS.Mode, buf::LCS.Buffer, state::LCS.State, config::B200
     LCS.evolve!(state)
     (; flow=(; couple1=(; itr=Int(lg.couple1.itr), div=lg.couple1.div),
                couple2=(; itr=Int(lg.couple2.itr), div=lg.couple2.div),
-               forcing=isnan(lg.p) ? LCS.EMPTY_LOG : (; p=lg.p)))
+               forcing=isnan(lg.p) ? LCS.EMPTY_LOG : isnan(lg.e10) ? (; p=lg.p) : (; p=lg.p, e10=lg.e10)))
 end
 
 # statistics and restart files read the reference's buffers: refresh them first
 function LCS.stat(buf::LCS.Buffer, state::LCS.State, config::B200Config, topo::Topologies.Topology)
     download!(buf, state, config)
     invoke(LCS.stat, Tuple{LCS.Buffer,LCS.State,LCS.Config,Topologies.Topology}, buf, state, config, topo)
+end
+
+# src/LCSIO/save.jl:40-43: a restart step need not be a statistics step
+function LCS.LCSIO.saverestart(buf::LCS.Buffer, state::LCS.State, config::B200Config, topo::Topologies.Topology)
+    download!(buf, state, config)
+    invoke(LCS.LCSIO.saverestart, Tuple{LCS.Buffer,LCS.State,LCS.Config,Topologies.Topology}, buf, state, config, topo)
 end
 
 end # module LCSB200

@@ -118,9 +118,15 @@ __device__ __forceinline__ void fill_halo_body(const Ctx* __restrict__ ctx, cons
       i = ii < r ? 1 - r + ii : nx + 1 + (ii - r);
     }
     const int64_t dst = g.at(i, j, k), src = g.at(wrap1(i, nx), wrap1(j, ny), wrap1(k, nz));
+    // every source is an interior cell and every destination a halo cell:
+    // all loads go out before the stores
+    T v[4];
 #pragma unroll
     for (int q = 0; q < 4; q++)
-      if (q < fa.nf) f[q][dst] = f[q][src];
+      if (q < fa.nf) v[q] = f[q][src];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (q < fa.nf) f[q][dst] = v[q];
   }
 }
 template <typename T>

@@ -194,14 +194,38 @@ def simulate(config, *, steps: int | None = None, quiet: bool = False, engine_cl
     return eng, logs
 
 
-def main(argv=None):
-    """`julia simulate.jl cfg.lcs-yaml` equivalent: python -m lcs_b200 cfg.lcs-yaml"""
+def main(argv=None, engine_cls=Engine):
+    """`julia simulate.jl cfg.lcs-yaml` equivalent: python -m lcs_b200 cfg.lcs-yaml [steps].
+
+    As LCSIO.init does (LCSIO/config.jl:30-76): a fresh run needs a new output
+    directory and saves the config there as config.lcs-yaml; an existing one
+    is resumed only with LCS_RESUME=1, and only if it holds restart files and
+    that config.  Statistics and restart files are written at their intervals."""
+    import os
+
+    import yaml
+
     argv = sys.argv[1:] if argv is None else argv
     if not argv:
         print("usage: python -m lcs_b200 <config.lcs-yaml> [steps]", file=sys.stderr)
         return 2
     steps = int(argv[1]) if len(argv) > 1 else None
-    simulate(argv[0], steps=steps)
+    rc = readconfig(argv[0])
+    out = rc.outdir
+    resume = os.environ.get("LCS_RESUME", "0").lower() in ("1", "true", "yes")
+    if os.path.isdir(out):
+        if not resume:
+            raise ValueError(f"output directory {out} already exists, set LCS_RESUME=1 to resume")
+        if latest_restart(out)[0] is None or not os.path.isfile(os.path.join(out, "config.lcs-yaml")):
+            raise ValueError(f"output directory {out} exists but is not resumable, "
+                             "missing restart files or config.lcs-yaml")
+    else:
+        resume = False
+        os.makedirs(out)
+        with open(os.path.join(out, "config.lcs-yaml"), "w") as f:
+            yaml.safe_dump(rc.raw, f, sort_keys=False)
+    eng, _ = simulate(rc, steps=steps, engine_cls=engine_cls, save=True, outdir=out, resume=resume)
+    eng.close()
     return 0
 
 

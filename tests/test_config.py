@@ -240,3 +240,30 @@ def test_restart_and_upsample_inits(tmp_path):
         assert np.array_equal(a, b)
     for e in (eng, again, fine, ref):
         e.close()
+
+
+def test_command_line_run_and_resume(tmp_path, monkeypatch, capsys):
+    """python -m lcs_b200 cfg [steps]: a fresh output directory with the
+    config saved, refusal of an existing one without LCS_RESUME, and a resume."""
+    from lcs_b200 import restart
+    from lcs_b200.simulate import main
+    from oracle_engine import load_oracle
+
+    d = small_run(steps=4, interval=2)
+    d["simulate"].update({"interval_restart": 2, "num_restart_files": 1})
+    out = tmp_path / "out"
+    d["outdir"] = str(out)
+    cfg = tmp_path / "run.lcs-yaml"
+    cfg.write_text(yaml.safe_dump(d))
+    monkeypatch.delenv("LCS_RESUME", raising=False)
+    assert main([str(cfg), "2"], engine_cls=OracleEngine) == 0
+    assert sorted(os.listdir(out)) == ["config.lcs-yaml", "restart.h5.2", "stat.h5"]
+    assert yaml.safe_load((out / "config.lcs-yaml").read_text())["simulate"]["last_step"] == 4
+    with pytest.raises(ValueError, match="LCS_RESUME"):
+        main([str(cfg)], engine_cls=OracleEngine)
+    monkeypatch.setenv("LCS_RESUME", "1")
+    assert main([str(cfg)], engine_cls=OracleEngine) == 0  # steps 3 and 4
+    assert sorted(os.listdir(out)) == ["config.lcs-yaml", "restart.h5.4", "stat.h5"]
+    assert restart.listing(load_oracle(), str(out / "stat.h5")) == ["2", "4"]
+    lines = [x for x in capsys.readouterr().out.splitlines() if x.startswith("step=")]
+    assert [x.split()[0] for x in lines] == ["step=1", "step=2", "step=3", "step=4"]

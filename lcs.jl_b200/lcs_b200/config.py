@@ -4,7 +4,9 @@ The YAML schema is the reference's (kind-tagged ``{"kind": ..., "params":
 ...}`` objects, lib/polyserde/src/PolySerde.jl:35-80; field names of
 src/config.jl, src/flows/config.jl, src/particles/config.jl).  The backend kind
 ``b200`` is new; its optional params are ``precision`` ("fp64" or
-"fp32-mixed"), ``device`` and ``graphs``.
+"fp32-mixed"), ``device``, ``graphs`` and ``particle_sort`` (sort the particles
+by cell every that many steps: lcs_set_particle_sort with the first species'
+cell grid_ratio; 0 or absent: off).
 
 New init kinds (no reference counterpart, generated on the host):
   flow.init "spectral"      params {seed, urms, kpeak}
@@ -70,6 +72,7 @@ class RunConfig:
     species: list = field(default_factory=list)
     last_step: int = 0
     interval_stat: int = 1
+    particle_sort: int = 0          # backend param: lcs_set_particle_sort interval (0: off)
     interval_restart: int = 0       # 0: no restart files
     num_restart_files: int = 1
     outdir: str = "output"
@@ -165,7 +168,7 @@ def from_dict(d: dict) -> RunConfig:
                      last_step=int(sim.get("last_step", 0)), interval_stat=int(sim.get("interval_stat", 1)),
                      interval_restart=int(sim.get("interval_restart", 0)),
                      num_restart_files=int(sim.get("num_restart_files", 1)), outdir=str(d.get("outdir", "output")),
-                     raw=d)
+                     particle_sort=int(bparams.get("particle_sort", 0) or 0), raw=d)
 
 
 def readconfig(path: str) -> RunConfig:

@@ -66,6 +66,8 @@ def init_engine(rc: RunConfig, engine_cls=Engine) -> Engine:
             eng.init_particle_velocity(s)
         elif si.velocity not in ("rest", "restart"):
             raise ValueError(f"particle velocity init {si.velocity!r} is not available")
+    if rc.particle_sort > 0 and rc.species:
+        eng.set_particle_sort(rc.particle_sort, rc.species[0].grid_ratio)
     return eng
 
 

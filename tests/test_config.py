@@ -267,3 +267,26 @@ def test_command_line_run_and_resume(tmp_path, monkeypatch, capsys):
     assert restart.listing(load_oracle(), str(out / "stat.h5")) == ["2", "4"]
     lines = [x for x in capsys.readouterr().out.splitlines() if x.startswith("step=")]
     assert [x.split()[0] for x in lines] == ["step=1", "step=2", "step=3", "step=4"]
+
+
+def test_backend_particle_sort_param():
+    """backend.params.particle_sort: the run sorts its particles by cell and
+    each particle (by id) and the flow equal the unsorted run's."""
+    d = small_run(steps=2, interval=5)
+    plain, _ = simulate(d, quiet=True, engine_cls=OracleEngine)
+    d["backend"]["params"]["particle_sort"] = 1
+    for p in d["particles"]:
+        p["cell"] = {"grid_ratio": 4}
+    rc = lcfg.from_dict(d)
+    assert rc.particle_sort == 1
+    sorted_, _ = simulate(rc, quiet=True, engine_cls=OracleEngine)
+    for a, b in zip(plain.download_flow(), sorted_.download_flow()):
+        assert np.array_equal(a, b)
+    for s in range(2):
+        pa, pb = plain.download_particles(s), sorted_.download_particles(s)
+        assert not np.array_equal(pa["ids"], pb["ids"])
+        oa, ob = np.argsort(pa["ids"]), np.argsort(pb["ids"])
+        for k in pa:
+            assert np.array_equal(pa[k][oa], pb[k][ob]), (s, k)
+    plain.close()
+    sorted_.close()

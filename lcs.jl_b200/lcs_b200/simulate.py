@@ -146,17 +146,18 @@ def simulate(config, *, steps: int | None = None, quiet: bool = False, engine_cl
     every interval_restart steps the state into `<outdir>/restart.h5.<step>`,
     keeping the last num_restart_files of them (LCSIO.cleanrestart).
 
-    resume (default: the LCS_RESUME environment variable, as LCSIO.init reads
-    it): continue from the latest restart.h5.<step> in outdir, with t from
-    stat.h5 (LCSIO.load_resume_state!), up to step last_step."""
+    resume (default with save=True: the LCS_RESUME environment variable, as
+    LCSIO.init reads it; otherwise False): continue from the latest
+    restart.h5.<step> in outdir, with t from stat.h5
+    (LCSIO.load_resume_state!), up to step last_step."""
     import os
 
     from . import restart
 
     rc = config if isinstance(config, RunConfig) else (readconfig(config) if isinstance(config, str) else from_dict(config))
     out = outdir or rc.outdir
-    if resume is None:
-        resume = os.environ.get("LCS_RESUME", "0").lower() in ("1", "true", "yes")
+    if resume is None:  # the environment decides only for runs that write their outputs
+        resume = save and os.environ.get("LCS_RESUME", "0").lower() in ("1", "true", "yes")
     start = 0
     if resume:
         file, start = latest_restart(out)

@@ -259,3 +259,21 @@ def test_stat_file_with_many_steps(tmp_path):
     with pytest.raises(Exception):
         restart.save_state(lib, junk, 1, 0.0, 0.0)
     assert open(junk, "rb").read() == b"x" * 1000
+
+
+def test_stat_save_rejects_bad_counts(tmp_path):
+    lib = load_oracle()
+    path = str(tmp_path / "stat.h5")
+    bad = _abi.ParticleStats()
+    bad.nbins = _abi.RDF_MAX_BINS + 1
+    with pytest.raises(Exception) as exc:
+        restart.save_stat(lib, path, 1, 0.0, 0.0, particles=[bad], nvalid=[1])
+    assert getattr(exc.value, "code", None) == _abi.EINVAL and not os.path.exists(path)
+    bad.nbins, bad.nshells = 4, _abi.SPECTRUM_MAX_SHELLS + 1
+    with pytest.raises(Exception):
+        restart.save_stat(lib, path, 1, 0.0, 0.0, particles=[bad], nvalid=[1])
+    assert lib.lcs_stat_save(path.encode(), 1, 0.0, 0.0, None, _abi.MAX_SPECIES + 1, None, None, None) == _abi.EINVAL
+    assert lib.lcs_stat_save(None, 1, 0.0, 0.0, None, 0, None, None, None) == _abi.EINVAL
+    # everything optional: the state entries alone
+    restart.save_stat(lib, path, 5, 1.5, 0.5)
+    assert restart.listing(lib, path, "5") == ["stat", "state"] and restart.load_state(lib, path, 5) == (1.5, 0.5)

@@ -209,8 +209,10 @@ def test_timestep_bitwise():
 
 
 @pytest.mark.parametrize("forcing", [F.FORCING_LINEAR_POWER, F.FORCING_RC_ENERGY])
-@pytest.mark.parametrize("n,coarse,kmax", [(16, 4, 2), (32, 8, 2), (32, 8, 3)])
+@pytest.mark.parametrize("n,coarse,kmax", [(16, 4, 2), (32, 8, 2), (32, 8, 3), (64, 4, 2), (256, 16, 2)])
 def test_forcing(forcing, n, coarse, kmax):
+    """Both forcings on random fields; (64, 4) and (256, 16) give the 16-cell
+    box filter of the rc256 workload (filter size n / coarse_size)."""
     cfg = make_config(n, mode=F.MODE_FLOW, forcing=forcing, power=0.5, energy=0.649, kmin=1, kmax=kmax,
                       coarse=coarse)
     g, o = pair(cfg)

@@ -1,25 +1,30 @@
 """Benchmark of the B200 time-step backend (LCS.jl hot path).
 
-Workload (default "rc256", the plain-FP64 256^3 configuration): periodic cube
-L = 2pi, 256^3 cells, nu = 0.005 (Re = 200), seeded solenoidal spectral init
-E(k) ~ k^4 exp(-2 (k/4)^2) with u_rms = 1, rc-energy forcing with a 16-cell
-box filter (coarse 16^3, kmin 1, kmax 2, e10 0.649), HSMAC red-black-fast with
-time blocking and overlap, omega 1.7, itrmin 6, itrmax 300, exit at RMS(div)
-< 1e-8, CFL 0.3, dtmax 0.01, and 2^20 Stokes particles in 2 species
-(tau_p = 0.05, 0.5; density ratio 843; velocity = interpolated fluid velocity).
+Default workload "lp512": periodic cube L = 2pi, 512^3 cells, nu = 0.0025
+(Re = 400), seeded solenoidal spectral init E(k) ~ k^4 exp(-2 (k/4)^2) with
+u_rms = 1, linear-power forcing P = 0.5, HSMAC red-black-fast with time
+blocking and overlap, omega 1.7, itrmin 6, itrmax 300, exit at RMS(div) <
+1e-8, CFL 0.3, dtmax 0.01, and 2^24 Stokes particles in 3 species (tau_p =
+0.02, 0.2, 2.0; density ratio 843; velocity = interpolated fluid velocity).
 
 A step is LCS.timestep! + LCS.evolve! over the whole grid and all particles.
-`value` is Mcell-steps/s (cells x steps / device seconds of the timed steps,
-max over ranks); particle-steps/s is reported beside it.  Every field is a
-(n+6)^3 FP64 array of 144 MB, so the inputs exceed the 126 MB L2 and no L2
-flush is needed between steps.
+The plain FP64 method is timed first: `value` is its Mcell-steps/s (cells x
+steps / device seconds of the timed steps, max over ranks), particle-steps/s
+beside it.  The FP32-mixed form then runs the same workload from the same
+inputs for the same warm-up and timed steps (`precision_forms`), and its
+state is compared with the FP64 state after those steps: relative L2 error
+per field, relative error per flow statistic (Flows.stat on the device), per
+E(k) shell and per particle species.  Every field is a (n+6)^3 array of
+1.1 GB (FP64), so the inputs exceed the 126 MB L2 and no flush is needed
+between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload rc256|lp128|lp512]
+                  [--workload lp512|rc256|lp128|batch64|serve|makeindex|couple256]
+                  [--precision fp64|fp32-mixed] [--no-forms] [--no-cpu-baseline]
 
 --impl reference times the CPU restatement of the reference (oracle/, the
 port of LCSCPU: the reference is Julia and cannot run here) on the host's
-cores over a bounded number of steps of the same workload.
+cores, each step a bounded sample of the same workload (below).
 """
 
 from __future__ import annotations
@@ -41,48 +46,25 @@ import numpy as np  # noqa: E402
 
 from lcs_b200 import config as lcfg  # noqa: E402
 from lcs_b200 import inits  # noqa: E402
+from lcs_b200.workloads import WORKLOADS, host_inputs, load_engine, make_run_config  # noqa: E402
 
-WORKLOADS = {
-    # the plain FP64 method at 256^3 with rc-energy forcing (the default bench workload)
-    "rc256": dict(n=256, nu=0.005, forcing={"kind": "rc-energy", "params": {"kmin": 1, "kmax": 2, "energy": 0.649,
-                                                                            "coarse_size": 16}},
-                  taups=[0.05, 0.5], counts=[2 ** 19, 2 ** 19], precision="fp64"),
-    # the CPU-runnable case: 128^3, linear-power P = 0.5, 65,536 particles tau_p = 0.1
-    "lp128": dict(n=128, nu=0.01, forcing={"kind": "linear-power", "params": {"power": 0.5}}, taups=[0.1],
-                  counts=[65536], precision="fp64"),
-    # the precision-form workload: 512^3, linear-power, 2^24 particles in 3 species
-    # (--precision selects the form; --report precision compares both)
-    "lp512": dict(n=512, nu=0.0025, forcing={"kind": "linear-power", "params": {"power": 0.5}},
-                  taups=[0.02, 0.2, 2.0], counts=[2 ** 24 // 3, 2 ** 24 // 3, 2 ** 24 - 2 * (2 ** 24 // 3)],
-                  precision="fp64"),
-    # the 64-member ensemble and the served request stream: run_batch and run_serve
-    "batch64": None,
-    "serve": None,
-    # the particle cell index (makeindex!) of the lp512 particles, grid_ratio 4: run_makeindex
-    "makeindex": None,
-    # one HSMAC couple of the rc256 fields with a fixed sweep count (the sweep
-    # kernels alone, for profiling): run_couple
-    "couple256": None,
-}
+# workloads with a run function of their own
+OTHER_WORKLOADS = ("batch64", "serve", "makeindex", "couple256")
 
-# DRAM bytes (read + write) per launch of the sweep kernel, per interior cell:
-# dram__bytes_read.sum + dram__bytes_write.sum of two launches captured by
-# `ncu --set full --clock-control none -k regex:hsmac_rw -s 50 -c 2` on
-# `python bench.py --steps 1 --warmup 0 --no-cpu-baseline` (rc256), averaged:
-# 1135.9 MB and 1200.2 MB per launch over 256^3 cells.
-SWEEP_DRAM_BYTES_PER_CELL = {"hsmac_rw": 69.6}
-# the FP32 form: 588.8 MB and 629.6 MB per launch (profiles/hsmac_rw_fp32_rc256.md)
-SWEEP_DRAM_BYTES_PER_CELL_FP32 = {"hsmac_rw": 36.3}
+# DRAM bytes (read + write) per interior cell of one launch of the sweep
+# kernel, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
+# of two sweep launches at 256^3: not measured in the run that reports them.
+SWEEP_DRAM_BYTES_PER_CELL = {"fp64": 69.6, "fp32-mixed": 36.3}
 SWEEP_KERNELS = ("hsmac_rw", "hsmac_tma", "hsmac_fused")
 # FP64 operations per interior cell of one rhs!+update! launch (k_rhs, both
 # stages alike): smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on
-# of `ncu ... -k regex:k_rhs -c 2` on the lp128 workload (profiles/rhs_lp128.md):
-# 484.4 M adds + 471.9 M multiplies, no FMA (the library is built without
-# contraction), over 128^3 cells.
+# of an ncu capture of k_rhs at 128^3: 484.4 M adds + 471.9 M multiplies, no
+# FMA (the FP64 library is built without contraction), over 128^3 cells.
 RHS_FLOPS_PER_CELL = 456.0
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+TWO_PI = 2.0 * math.pi
 
 
 def hbm_peak():
@@ -91,62 +73,6 @@ def hbm_peak():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
-
-
-def make_run_config(name, seed=0, precision=None):
-    w = WORKLOADS[name]
-    d = lcfg.workload(w["n"], w["nu"], w["forcing"], w["taups"], w["counts"], seed=seed,
-                      precision=precision or w["precision"])
-    return lcfg.from_dict(d), w
-
-
-def time_form(workload, precision, steps, seed, device):
-    """Device time of `steps` graph-replayed steps of another precision form on
-    the same workload and inputs (after one warm-up step)."""
-    from lcs_b200 import Engine
-
-    rc, w = make_run_config(workload, seed=seed, precision=precision)
-    rc.abi.device = device
-    rc.abi.use_graphs = 1
-    flow, parts = host_inputs(rc, pinned=False)
-    eng = Engine(rc.abi)
-    load_engine(eng, rc, flow, parts)
-    eng.step(1)
-    eng.synchronize()
-    _, ms = eng.step_timed(steps)
-    eng.close()
-    return ms
-
-
-def host_inputs(rc, pinned=False):
-    """Seeded initial state on the host (optionally in pinned memory)."""
-    n = rc.dims[0]
-    p = rc.flow_init_params
-    U, V, W, P = inits.spectral_flow(n, seed=int(p.get("seed", 0)), urms=1.0, kpeak=4.0)
-    parts = []
-    for s, si in enumerate(rc.species):
-        x, y, z = inits.random_positions(si.nvalid, si.position_seed)
-        parts.append((np.full(si.nvalid, si.diam), x, y, z))
-    if pinned:
-        import torch
-
-        def pin(a):
-            t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
-            t.numpy()[...] = a
-            return t.numpy()
-
-        U, V, W, P = (pin(a) for a in (U, V, W, P))
-        parts = [tuple(pin(a) for a in sp) for sp in parts]
-    return (U, V, W, P), parts
-
-
-def load_engine(eng, rc, flow, parts):
-    eng.upload_flow(*flow)
-    for s, (d, x, y, z) in enumerate(parts):
-        zero = np.zeros_like(x)
-        eng.upload_particles(s, d, x, y, z, zero, zero, zero)
-        if rc.species[s].velocity == "interp":
-            eng.init_particle_velocity(s)
 
 
 class ClockSampler:
@@ -232,79 +158,75 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_baseline(rc, w, budget_s=30.0):
-    """The oracle (C restatement of the reference, OpenMP over all host cores)
-    on a bounded number of steps of the same workload."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from oracle_engine import OracleEngine, load_oracle
-
-    flow, parts = host_inputs(rc)
-    eng = OracleEngine(rc.abi)
-    load_engine(eng, rc, flow, parts)
-    cores = load_oracle().lcs_oracle_threads()
-    steps = 0
-    t0 = time.perf_counter()
-    while True:
-        eng.step(1)
-        steps += 1
-        el = time.perf_counter() - t0
-        if el * (steps + 1) / steps > budget_s or steps >= 100:
-            break
-    el = time.perf_counter() - t0
-    n3 = float(np.prod(rc.dims))
-    np_tot = sum(w["counts"])
-    eng.close()
-    return {"value": n3 * steps / el / 1e6, "unit": "Mcell-steps/s", "cores": cores, "kind": "port",
-            "sample": f"{steps} full step(s) of the {rc.dims[0]}^3 workload ({el:.1f} s)",
-            "particle_steps_per_s": np_tot * steps / el, "seconds": el, "steps": steps}
 
 
-def run_reference(args):
-    """Rank 0 alone times the CPU restatement; other ranks exit without work."""
-    rank = int(os.environ.get("RANK", "0"))
-    rc, w = make_run_config(args.workload)
-    line = None
-    if rank == 0:
-        base = cpu_baseline(rc, w, budget_s=float(os.environ.get("LCS_REFERENCE_BUDGET_S", "150")))
-        line = {"metric": "Mcell-steps/s", "value": base["value"], "unit": "Mcell-steps/s", "n_gpus": args.gpus,
-                "steps": base["steps"], "warmup": 0, "ms_per_step": base["seconds"] * 1e3 / base["steps"],
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded spectral field, uniform random particles)",
-                "config": {"workload": args.workload, "n": rc.dims[0], "particles": sum(w["counts"]),
-                           "species": len(w["counts"]), "parallelism": "replicas"},
-                "impl": "reference",
-                "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
-                "e2e": {"value": base["value"], "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0},
-                "particle_steps_per_s": base["particle_steps_per_s"]}
-        print(json.dumps(line), flush=True)
-    return 0
+def elem_bytes(precision):
+    return 4 if precision == "fp32-mixed" else 8
 
 
-def run_b200(args):
-    world, rank, local = dist_setup()
+def kernel_table(tot, n, h, T, particles_per_launch, peak):
+    """Per-kernel device ms and launches of the profiled steps, with the HBM
+    fraction of every kernel that has a byte model (kernel_bytes)."""
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in sorted(tot.items(), key=lambda kv: -kv[1][0])}
+    for k, alg in kernel_bytes(n, h, T, particles_per_launch).items():
+        if k in kernels and kernels[k]["launches"]:
+            ms_l = kernels[k]["ms"] / kernels[k]["launches"]
+            gbs = alg / (ms_l / 1e3) / 1e9
+            kernels[k].update({"alg_bytes_per_launch": alg, "gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 3)})
+    return kernels
+
+
+def sweep_roofline(tot, n3, precision, peak, peak_kind):
+    """HBM roofline of the dominant kernel, the fused red-black sweep: 8T bytes
+    per interior cell (U, V, W, P read and written once) over its average
+    CUDA-event launch time."""
+    k = max(SWEEP_KERNELS, key=lambda s: tot.get(s, (0.0, 0))[0])
+    ms, cnt = tot.get(k, (0.0, 0))
+    T = elem_bytes(precision)
+    alg = 8 * T * n3
+    avg = ms / max(cnt, 1)
+    ach = alg / (avg / 1e3) / 1e9 if cnt else None
+    return {"kernel": k, "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": (ach / peak) if ach else None, "traffic": SWEEP_DRAM_BYTES_PER_CELL[precision] * n3,
+            "traffic_source": "not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum per "
+                              f"interior cell of a 256^3 capture of the same kernel "
+                              f"({SWEEP_DRAM_BYTES_PER_CELL[precision]} B), times n^3",
+            "alg_bytes_per_launch": alg, "avg_launch_ms": avg, "launches_profiled": cnt}
+
+
+def run_form(args, precision, rc_w, flow, parts, world, device, primary):
+    """One precision form on the workload: W warm-up steps, K timed steps
+    (CUDA-graph replays, device-timed), the state after them downloaded, two
+    profiled steps (per-kernel CUDA events) and, for the primary form, the
+    end-to-end run through the per-step C-ABI calls with host buffers."""
+    import ctypes as C
+
     from lcs_b200 import Engine
 
-    rc, w = make_run_config(args.workload, seed=rank, precision=args.precision)
-    rc.abi.device = local if world > 1 else int(os.environ.get("LCS_DEVICE", "0"))
+    rc, w = rc_w
+    rc.abi.device = device
     rc.abi.use_graphs = 1
     n3 = float(np.prod(rc.dims))
     np_tot = float(sum(w["counts"]))
-    flow, parts = host_inputs(rc, pinned=True)
     eng = Engine(rc.abi)
     load_engine(eng, rc, flow, parts)
-    # warm-up (also builds the step graph)
-    eng.step(args.warmup)
+    eng.step(args.warmup)  # also builds the step graphs
     eng.synchronize()
     barrier(world)
-    with ClockSampler(rc.abi.device) as clk:
+    with ClockSampler(device) as clk:
         logs, ms = eng.step_timed(args.steps)
     barrier(world)
-    div_rms, div_max = eng.flow_divergence()  # of the state after the timed steps
     ms_max = reduce_max(ms, world)
-    value = world * n3 * args.steps / (ms_max / 1e3) / 1e6
-    pvalue = world * np_tot * args.steps / (ms_max / 1e3)
-    sweeps = [lg["couple1"]["sweeps"] + lg["couple2"]["sweeps"] for lg in logs]
+    res = {"value": world * n3 * args.steps / (ms_max / 1e3) / 1e6, "ms_per_step": ms_max / args.steps,
+           "particle_steps_per_s": world * np_tot * args.steps / (ms_max / 1e3), "clocks": clk.summary(),
+           "sweeps_per_step": statistics.mean(lg["couple1"]["sweeps"] + lg["couple2"]["sweeps"] for lg in logs),
+           "last_log": logs[-1], "after_steps": args.warmup + args.steps}
+    # the state after W + K steps, for the error of the FP32-mixed form
+    if not args.no_forms:
+        res["flow"] = eng.download_flow()
+        res["parts"] = [eng.download_particles(s) for s in range(len(parts))]
+        res["stat"] = eng.flow_stat()
+    res["divergence"] = eng.flow_divergence()
 
     # per-kernel device times from CUDA events around every launch (same stream)
     eng.profile(True)
@@ -313,159 +235,62 @@ def run_b200(args):
     eng.step(prof_steps)
     tot = eng.profile_totals()
     eng.profile(False)
-    # kernel launches per step, counted on the launch-by-launch (profiled) path;
-    # the graph replays the same kernels with the same loop counts
-    launches = int(round(sum(v[1] for v in tot.values()) / prof_steps * args.steps))
-    # the dominant kernel: the fused red-black sweep (TMA-fed, or the plain form)
-    sweep_kernel = max(SWEEP_KERNELS, key=lambda k: tot.get(k, (0.0, 0))[0])
-    ms_sweep, cnt = tot.get(sweep_kernel, (0.0, 0))
-    T = 4 if args.precision == "fp32-mixed" else 8  # bytes per field element
+    res["launches_per_step"] = sum(v[1] for v in tot.values()) / prof_steps
     peak, peak_kind = hbm_peak()
-    alg_bytes = 8 * T * n3  # U, V, W, P read and written once per interior cell per sweep
-    avg_ms = ms_sweep / max(cnt, 1)
-    achieved = alg_bytes / (avg_ms / 1e3) / 1e9 if cnt else None
-    traffic = (SWEEP_DRAM_BYTES_PER_CELL_FP32 if T == 4 else SWEEP_DRAM_BYTES_PER_CELL).get(sweep_kernel)
-    traffic = traffic * n3 if traffic else None
-    kernels = {k: {"ms": round(v[0], 3), "launches": v[1]} for k, v in sorted(tot.items(), key=lambda kv: -kv[1][0])}
-    # FP64 roofline of rhs! + update!: the measured FMA peak of this GPU
-    import ctypes as C
+    T = elem_bytes(precision)
+    res["roofline"] = sweep_roofline(tot, n3, precision, peak, peak_kind)
+    res["kernels"] = kernel_table(tot, int(rc.dims[0]), int(rc.abi.halo_size), T, np_tot / max(1, len(rc.species)),
+                                  peak)
+    if precision == "fp64":
+        fp64_peak = C.c_double()
+        if eng.lib.lcs_measure_fp64_peak(device, C.byref(fp64_peak)) == 0 and "rhs_update" in tot:
+            ms_r, cnt_r = tot["rhs_update"]
+            tf = RHS_FLOPS_PER_CELL * n3 / (ms_r / cnt_r / 1e3) / 1e12
+            res["fp64"] = {"peak_tflops": round(fp64_peak.value, 2), "peak_kind": "measured (k_fp64_peak, FMA chains)",
+                           "rhs_flops_per_cell": RHS_FLOPS_PER_CELL, "rhs_tflops": round(tf, 2),
+                           "rhs_frac": round(tf / fp64_peak.value, 3),
+                           "note": "rhs has no FMA (no contraction): add/multiply issue at half the FMA rate"}
 
-    fp64_peak = C.c_double()
-    fp64 = None
-    if args.precision == "fp64" and eng.lib.lcs_measure_fp64_peak(rc.abi.device, C.byref(fp64_peak)) == 0 \
-            and "rhs_update" in tot:
-        ms_r, cnt_r = tot["rhs_update"]
-        tf = RHS_FLOPS_PER_CELL * n3 / (ms_r / cnt_r / 1e3) / 1e12
-        fp64 = {"peak_tflops": round(fp64_peak.value, 2), "peak_kind": "measured (k_fp64_peak, FMA chains)",
-                "rhs_flops_per_cell": RHS_FLOPS_PER_CELL, "rhs_tflops": round(tf, 2),
-                "rhs_frac": round(tf / fp64_peak.value, 3),
-                "note": "rhs has no FMA (no contraction): add/multiply issue at half the FMA rate"}
-    # HBM-roofline fraction of every kernel with a byte model (algorithmic
-    # bytes per launch; the profiled steps' CUDA-event averages)
-    n_ = int(rc.dims[0])
-    for k, alg in kernel_bytes(n_, int(rc.abi.halo_size), T, np_tot / max(1, len(rc.species))).items():
-        if k in kernels and kernels[k]["launches"]:
-            ms_l = kernels[k]["ms"] / kernels[k]["launches"]
-            gbs = alg / (ms_l / 1e3) / 1e9
-            kernels[k].update({"alg_bytes_per_launch": alg, "gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 3)})
+    if primary:
+        # end to end through the public API: pinned host state in, the per-step
+        # timestep!/evolve! calls of the Julia shim, state out into pinned memory
+        import torch
 
-    # end to end through the public API: pinned host state in, the per-step
-    # timestep!/evolve! calls of the Julia shim, state out
-    h2d0, d2h0 = eng.transfer_stats()
-    e2e_steps = max(1, min(args.steps, 5))
-    import torch
+        def pinned_empty(shape):
+            return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
 
-    def pinned_empty(shape):  # the result lands in pinned host memory, as the inputs come from it
-        return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
-
-    out_flow = [pinned_empty(eng.interior_shape) for _ in range(4)]
-    out_parts = []
-    for si in rc.species:
-        ids = torch.empty(si.nvalid, dtype=torch.int64, pin_memory=True).numpy()
-        out_parts.append((ids, [pinned_empty(si.nvalid) for _ in range(7)]))
-    barrier(world)
-    t0 = time.perf_counter()
-    load_engine(eng, rc, flow, parts)
-    for _ in range(e2e_steps):
-        dt = eng.timestep()
-        eng.evolve(dt)
-    import ctypes as C
-
-    eng._check(eng.lib.lcs_download_flow(eng.handle, *[a.ctypes.data_as(C.POINTER(C.c_double)) for a in out_flow]))
-    for s, (out_ids, out_p) in enumerate(out_parts):
-        eng._check(eng.lib.lcs_download_particles(eng.handle, s, out_ids.ctypes.data_as(C.POINTER(C.c_int64)),
-                                                  *[a.ctypes.data_as(C.POINTER(C.c_double)) for a in out_p]))
-    eng.synchronize()
-    e2e_s = reduce_max(time.perf_counter() - t0, world)
-    h2d1, d2h1 = eng.transfer_stats()
-    e2e_value = world * n3 * e2e_steps / e2e_s / 1e6
-    eng.close()
-
-    # the other precision form on the same workload and seed (FP32-mixed beside FP64)
-    forms = None
-    if not args.no_forms:
-        other = "fp32-mixed" if args.precision == "fp64" else "fp64"
-        k = max(1, min(args.steps, 5))
-        ms_o = reduce_max(time_form(args.workload, other, k, rank, rc.abi.device), world)
-        v_o = world * n3 * k / (ms_o / 1e3) / 1e6
-        forms = {args.precision: {"value": value, "ms_per_step": ms_max / args.steps},
-                 other: {"value": v_o, "ms_per_step": ms_o / k, "steps": k}}
-        forms["fp32_mixed_vs_fp64"] = forms["fp32-mixed"]["value"] / forms["fp64"]["value"]
-
-    base = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(rc, w, budget_s=float(os.environ.get("LCS_CPU_BUDGET_S", "25")))
-    if rank == 0:
-        line = {
-            "metric": "Mcell-steps/s",
-            "value": value,
-            "unit": "Mcell-steps/s",
-            "n_gpus": world,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True,
-            "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32 (FP64 residuals, reductions, positions)",
-            "data": "synthetic (seeded spectral field, uniform random particles)",
-            "config": {"workload": args.workload, "n": rc.dims[0], "particles": int(np_tot),
-                       "species": len(w["counts"]), "forcing": w["forcing"]["kind"], "hsmac_itrmax": 300,
-                       "hsmac_rms_div_tol": 1e-8, "l2": "inputs larger than L2 (144 MB per field)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "precision": args.precision},
-            "particle_steps_per_s": pvalue,
-            "hsmac_sweeps_per_step": statistics.mean(sweeps) if sweeps else None,
-            "gpu_launches": int(launches),
-            "clocks": clk.summary(),
-            "roofline": {"kernel": sweep_kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum",
-                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms},
-            "kernels": kernels,
-            "fp64": fp64,
-            "divergence": {"rms": div_rms, "max": div_max, "last_couple_residual": logs[-1]["couple2"]["div"],
-                           "note": "of the velocity after the timed steps, HSMAC form, interior cells"},
-            "e2e": {"value": e2e_value, "unit": "Mcell-steps/s",
-                    "h2d_bytes_per_step": (h2d1 - h2d0) / e2e_steps, "d2h_bytes_per_step": (d2h1 - d2h0) / e2e_steps,
-                    "steps": e2e_steps, "path": "upload + per-step lcs_timestep/lcs_evolve + download"},
-            "cpu_baseline": ({k: base[k] for k in ("value", "unit", "cores", "kind", "sample")} if base else None),
-            "precision_forms": forms,
-        }
-        print(json.dumps(line), flush=True)
-    barrier(world)
-    return 0
-
-
-# ---------------------------------------------------------------- precision report
-def run_precision_report(args):
-    """The precision-form workload: the FP32-mixed form against the plain FP64 form
-    on the same workload and seed after --steps steps: throughput of both, and
-    the FP32-mixed error per field (rel-L2 of U, V, W, P), per flow statistic
-    (urms, epsilon, Re_lambda, skewness of the restated Flows.stat), per E(k)
-    shell, and per particle species (rms velocity)."""
-    from lcs_b200 import Engine, stats
-
-    res = {}
-    for prec in ("fp64", "fp32-mixed"):
-        rc, w = make_run_config(args.workload, seed=0, precision=prec)
-        rc.abi.use_graphs = 1
-        flow, parts = host_inputs(rc)
-        eng = Engine(rc.abi)
+        h2d0, d2h0 = eng.transfer_stats()
+        e2e_steps = max(1, min(args.steps, 5))
+        out_flow = [pinned_empty(eng.interior_shape) for _ in range(4)]
+        out_parts = []
+        for si in rc.species:
+            ids = torch.empty(si.nvalid, dtype=torch.int64, pin_memory=True).numpy()
+            out_parts.append((ids, [pinned_empty(si.nvalid) for _ in range(7)]))
+        barrier(world)
+        t0 = time.perf_counter()
         load_engine(eng, rc, flow, parts)
-        eng.step(1)  # warm-up (graph build), then the timed steps
+        for _ in range(e2e_steps):
+            dt = eng.timestep()
+            eng.evolve(dt)
+        eng._check(eng.lib.lcs_download_flow(eng.handle, *[a.ctypes.data_as(C.POINTER(C.c_double)) for a in out_flow]))
+        for s, (out_ids, out_p) in enumerate(out_parts):
+            eng._check(eng.lib.lcs_download_particles(eng.handle, s, out_ids.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                      *[a.ctypes.data_as(C.POINTER(C.c_double)) for a in out_p]))
         eng.synchronize()
-        logs, ms = eng.step_timed(args.steps)
-        n3 = float(np.prod(rc.dims))
-        out_flow = eng.download_flow()
-        out_parts = [eng.download_particles(s) for s in range(len(parts))]
-        eng.close()
-        st = stats.flow_stat(*out_flow[:3], nu=w["nu"])
-        res[prec] = {"value": n3 * args.steps / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps,
-                     "sweeps_per_step": float(np.mean([lg["couple1"]["sweeps"] + lg["couple2"]["sweeps"] for lg in logs])),
-                     "flow": out_flow, "parts": out_parts, "stat": st,
-                     "spectrum": stats.energy_spectrum(*out_flow[:3])}
-    a, b = res["fp32-mixed"], res["fp64"]
+        e2e_s = reduce_max(time.perf_counter() - t0, world)
+        h2d1, d2h1 = eng.transfer_stats()
+        res["e2e"] = {"value": world * n3 * e2e_steps / e2e_s / 1e6, "unit": "Mcell-steps/s",
+                      "h2d_bytes_per_step": (h2d1 - h2d0) / e2e_steps, "d2h_bytes_per_step": (d2h1 - d2h0) / e2e_steps,
+                      "steps": e2e_steps,
+                      "path": "pinned host state uploaded, per-step lcs_timestep/lcs_evolve, state downloaded into "
+                              "pinned memory (host wall clock, max over ranks)"}
+    eng.close()
+    return res
+
+
+def precision_errors(a, b, nu):
+    """The FP32-mixed state `a` against the FP64 state `b` after the same steps."""
+    from lcs_b200 import stats
 
     def rel(x, y):
         return float(abs(x - y) / abs(y)) if y != 0 else float(abs(x - y))
@@ -473,33 +298,190 @@ def run_precision_report(args):
     def rel_l2(x, y):
         return float(np.linalg.norm((x - y).ravel()) / np.linalg.norm(y.ravel()))
 
-    ek_b, ek_a = b["spectrum"], a["spectrum"]
+    ek_a = stats.energy_spectrum(*a["flow"][:3])
+    ek_b = stats.energy_spectrum(*b["flow"][:3])
     shells = [k for k in range(1, len(ek_b)) if ek_b[k] > 1e-12 * ek_b[1:].max()]
-    line = {
-        "metric": "Mcell-steps/s, FP32-mixed vs FP64", "workload": args.workload, "steps": args.steps,
-        "n": int(make_run_config(args.workload)[0].dims[0]),
-        "fp64": {k: b[k] for k in ("value", "ms_per_step", "sweeps_per_step")},
-        "fp32_mixed": {k: a[k] for k in ("value", "ms_per_step", "sweeps_per_step")},
-        "fp32_mixed_vs_fp64": a["value"] / b["value"],
-        "hsmac_epsp": "epsp = 1e-8 * dxmin in both forms (RMS div < 1e-8); neither reaches it, both run itrmax = 300",
-        "errors": {
-            "field_rel_l2": {f: rel_l2(x, y) for f, x, y in zip("UVWP", a["flow"], b["flow"])},
-            "stat_rel": {k: rel(a["stat"][k], b["stat"][k]) for k in ("urms", "k", "epsilon", "Re_lambda",
-                                                                     "skewness", "flatness")},
-            "spectrum_max_rel": max(rel(ek_a[k], ek_b[k]) for k in shells),
-            "spectrum_shells": len(shells),
-            "particle_rms_velocity_rel": [
-                rel(stats.particle_rms_velocity(pa["u"], pa["v"], pa["w"]),
-                    stats.particle_rms_velocity(pb["u"], pb["v"], pb["w"]))
-                for pa, pb in zip(a["parts"], b["parts"])],
-            "particle_position_rel_l2": [
-                float(np.sqrt(sum(np.sum((pa[k] - pb[k]) ** 2) for k in "xyz") / sum(np.sum(pb[k] ** 2) for k in "xyz")))
-                for pa, pb in zip(a["parts"], b["parts"])],
-        },
+    return {
+        "after_steps": b["after_steps"],
+        "field_rel_l2": {f: rel_l2(x, y) for f, x, y in zip("UVWP", a["flow"], b["flow"])},
+        "stat_rel": {k: rel(a["stat"][k], b["stat"][k]) for k in ("urms", "k", "epsilon", "Re_lambda", "skewness",
+                                                                 "flatness")},
+        "spectrum_max_rel": max(rel(ek_a[k], ek_b[k]) for k in shells),
+        "spectrum_shells": len(shells),
+        "particle_rms_velocity_rel": [
+            rel(stats.particle_rms_velocity(pa["u"], pa["v"], pa["w"]),
+                stats.particle_rms_velocity(pb["u"], pb["v"], pb["w"]))
+            for pa, pb in zip(a["parts"], b["parts"])],
+        "particle_position_rel_l2": [
+            float(np.sqrt(sum(np.sum((pa[k] - pb[k]) ** 2) for k in "xyz") / sum(np.sum(pb[k] ** 2) for k in "xyz")))
+            for pa, pb in zip(a["parts"], b["parts"])],
         "fp64_stat": {k: b["stat"][k] for k in ("urms", "epsilon", "Re_lambda", "skewness", "flatness")},
-        "data": "synthetic (seeded spectral field, uniform random particles)",
+        "note": "statistics: Flows.stat on the device (FP64 reductions) of each form's final state; E(k): "
+                "shell sums of 0.5|u_hat|^2; tolerance target for the velocity: rel-L2 <= 1e-4",
     }
+
+
+# ------------------------------------------------------------------ CPU baseline
+class OracleSample:
+    """The oracle (C restatement of the reference, OpenMP over all host cores)
+    on a bounded sample of the workload.
+
+    A full 512^3 oracle step takes minutes (its 600 HSMAC sweeps dominate), so
+    a step is measured in two parts: the step with each couple cut to one
+    time-blocked group of 3 sweeps (timestep!, both rhs!/update!, forcing!,
+    the particles, 2 x 3 sweeps) and one 3-sweep couple; the step time is the
+    first plus (S/3 - 2) times the second, S being the sweeps per step of the
+    GPU run of the same workload.  A couple of S/2 sweeps is S/6 such groups
+    (halo fill, the overlap sweep with its face phases, two plain sweeps)."""
+
+    def __init__(self, workload, flow, parts):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_engine import OracleEngine, load_oracle
+
+        rc, w = make_run_config(workload, precision="fp64", itrmax=3)
+        rc.abi.use_graphs = 0
+        self.n3 = float(np.prod(rc.dims))
+        self.np_tot = float(sum(w["counts"]))
+        self.cores = load_oracle().lcs_oracle_threads()
+        self.eng = OracleEngine(rc.abi)
+        load_engine(self.eng, rc, flow, parts)
+
+    def capped_step(self):
+        t0 = time.perf_counter()
+        dt = self.eng.timestep()
+        self.eng.evolve(dt)
+        self.dt = dt
+        return time.perf_counter() - t0
+
+    def group(self):
+        t0 = time.perf_counter()
+        self.eng.couple(2, self.dt)
+        return time.perf_counter() - t0
+
+    def close(self):
+        self.eng.close()
+
+
+def cpu_baseline(workload, flow, parts, sweeps_per_step):
+    smp = OracleSample(workload, flow, parts)
+    t_step3 = smp.capped_step()
+    t_group = smp.group()
+    smp.close()
+    t = t_step3 + (sweeps_per_step / 3.0 - 2.0) * t_group
+    return {"value": smp.n3 / t / 1e6, "unit": "Mcell-steps/s", "cores": smp.cores, "kind": "port",
+            "sample": f"one step of the {workload} workload with each couple cut to 3 sweeps ({t_step3:.1f} s) and "
+                      f"one 3-sweep couple ({t_group:.2f} s), extrapolated to {sweeps_per_step:.0f} sweeps per step "
+                      f"(the GPU run's count): {t:.1f} s per step",
+            "particle_steps_per_s": smp.np_tot / t, "seconds_per_step": t}
+
+
+def run_reference(args):
+    """Rank 0 alone times the CPU restatement; other ranks exit without work.
+    Warm-up: the capped step (whose non-sweep part is kept) and W 3-sweep
+    couples; each timed step: one 3-sweep couple, the step's time assembled as
+    in OracleSample."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if args.workload in OTHER_WORKLOADS:
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU arm for the {args.workload} workload"}))
+        return 0
+    rc, w = make_run_config(args.workload)
+    flow, parts = host_inputs(rc)
+    smp = OracleSample(args.workload, flow, parts)
+    t_step3 = smp.capped_step()
+    groups = [smp.group() for _ in range(max(1, args.warmup))]
+    S = float(os.environ.get("LCS_REFERENCE_SWEEPS", "600"))  # both couples run itrmax = 300
+    t_rest = t_step3 - 2.0 * groups[0]
+    times = [t_rest + S / 3.0 * smp.group() for _ in range(args.steps)]
+    smp.close()
+    total = sum(times)
+    value = smp.n3 * args.steps / total / 1e6
+    sample = (f"each step: one 3-sweep HSMAC couple timed, times {S / 3.0:.0f}, plus the non-sweep part of a step "
+              f"({t_rest:.1f} s, timed once in warm-up on a step with each couple cut to 3 sweeps)")
+    line = {"metric": "Mcell-steps/s", "value": value, "unit": "Mcell-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded spectral field, uniform random particles)",
+            "config": {"workload": args.workload, "n": rc.dims[0], "particles": sum(w["counts"]),
+                       "species": len(w["counts"]), "precision": "fp64", "parallelism": "replicas"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "Mcell-steps/s", "cores": smp.cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "particle_steps_per_s": smp.np_tot * args.steps / total}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    world, rank, local = dist_setup()
+    device = local if world > 1 else int(os.environ.get("LCS_DEVICE", "0"))
+    rc, w = make_run_config(args.workload, seed=rank, precision=args.precision)
+    flow, parts = host_inputs(rc, pinned=True)
+    n3 = float(np.prod(rc.dims))
+    main = run_form(args, args.precision, (rc, w), flow, parts, world, device, primary=True)
+
+    # the other precision form on the same workload, inputs and step counts
+    forms = None
+    if not args.no_forms:
+        other = "fp32-mixed" if args.precision == "fp64" else "fp64"
+        o = run_form(args, other, make_run_config(args.workload, seed=rank, precision=other), flow, parts, world,
+                     device, primary=False)
+        by = {args.precision: main, other: o}
+        forms = {p: {"value": r["value"], "ms_per_step": r["ms_per_step"], "sweeps_per_step": r["sweeps_per_step"],
+                     "roofline_frac": r["roofline"]["frac"], "sweep_avg_launch_ms": r["roofline"]["avg_launch_ms"],
+                     "clocks": r["clocks"]}
+                 for p, r in by.items()}
+        forms["fp32-mixed"]["kernels"] = by["fp32-mixed"]["kernels"]
+        forms["fp32_mixed_vs_fp64"] = by["fp32-mixed"]["value"] / by["fp64"]["value"]
+        forms["errors"] = precision_errors(by["fp32-mixed"], by["fp64"], w["nu"])
+        forms["hsmac_epsp"] = ("epsp = 1e-8 * dxmin in both forms (RMS div < 1e-8); the sweep counts per step are "
+                               "those above")
+        for r in by.values():
+            for k in ("flow", "parts"):
+                r.pop(k, None)
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload in WORKLOADS:
+        base = cpu_baseline(args.workload, flow, parts, main["sweeps_per_step"])
+    if rank == 0:
+        div_rms, div_max = main["divergence"]
+        line = {
+            "metric": "Mcell-steps/s",
+            "value": main["value"],
+            "unit": "Mcell-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": main["ms_per_step"],
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 (FP64 residuals, reductions, positions)",
+            "data": "synthetic (seeded spectral field, uniform random particles)",
+            "config": {"workload": args.workload, "n": rc.dims[0], "particles": int(sum(w["counts"])),
+                       "species": len(w["counts"]), "forcing": w["forcing"]["kind"], "hsmac_itrmax": 300,
+                       "hsmac_rms_div_tol": 1e-8,
+                       "l2": f"inputs larger than L2 ({(rc.dims[0] + 6) ** 3 * elem_bytes(args.precision) / 1e6:.0f} "
+                             "MB per field)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "precision": args.precision},
+            "particle_steps_per_s": main["particle_steps_per_s"],
+            "hsmac_sweeps_per_step": main["sweeps_per_step"],
+            "gpu_launches": int(round(main["launches_per_step"] * args.steps)),
+            "clocks": main["clocks"],
+            "roofline": main["roofline"],
+            "kernels": main["kernels"],
+            "fp64": main.get("fp64"),
+            "divergence": {"rms": div_rms, "max": div_max, "last_couple_residual": main["last_log"]["couple2"]["div"],
+                           "note": "of the velocity after the timed steps, HSMAC form, interior cells"},
+            "e2e": main["e2e"],
+            "cpu_baseline": ({k: base[k] for k in ("value", "unit", "cores", "kind", "sample")} if base else None),
+            "precision_forms": forms,
+        }
+        print(json.dumps(line), flush=True)
+    barrier(world)
     return 0
 
 
@@ -871,20 +853,16 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rc256")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + list(OTHER_WORKLOADS), default="lp512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "fp32-mixed"], default="fp64")
-    ap.add_argument("--no-forms", action="store_true", help="skip timing the other precision form")
-    ap.add_argument("--report", choices=["precision"], default=None,
-                    help="precision: FP32-mixed vs FP64 errors per field and statistic (config 2)")
+    ap.add_argument("--no-forms", action="store_true", help="skip the other precision form and its errors")
     ap.add_argument("--requests", type=int, default=1000, help="serve: number of requests")
     ap.add_argument("--steps-scale", type=float, default=1.0, help="serve: scale of the 50-500 step counts")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: mean arrivals per second")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.report == "precision":
-        return run_precision_report(args)
     if args.workload in ("batch64", "serve"):
         # one hardware work queue per member stream (read at context creation)
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")

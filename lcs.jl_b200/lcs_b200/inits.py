@@ -47,37 +47,62 @@ def spectral_flow(n: int, seed: int = 0, urms: float = 1.0, kpeak: float = 4.0, 
     ~ E(k)), and evaluated at the staggered points of each component --
     U at (i dx, (j-1/2) dy, (k-1/2) dz), V at ((i-1/2) dx, j dy, (k-1/2) dz),
     W at ((i-1/2) dx, (j-1/2) dy, k dz) (src/particles/interp.jl:92-126) --
-    by a phase shift before the inverse FFT.  The real part is kept and the
-    three components are scaled together so that sqrt(<U^2+V^2+W^2>/3) = urms.
-    Returns U, V, W, P (P = 0) indexed [k, j, i].
+    by a phase shift (a product of per-axis phases) before the inverse FFT.
+    The real part is kept and the three components are scaled together so
+    that sqrt(<U^2+V^2+W^2>/3) = urms.  Returns U, V, W, P (P = 0) indexed
+    [k, j, i].  The inverse FFTs use every host core when SciPy is present.
     """
+    import os
+
+    try:
+        import scipy.fft as sfft
+
+        def ifftn(a):
+            return sfft.ifftn(a, workers=os.cpu_count() or 1, overwrite_x=True)
+    except ImportError:  # numpy's FFT (one thread)
+        ifftn = np.fft.ifftn
     rng = np.random.default_rng(seed)
     k1 = np.fft.fftfreq(n, d=1.0 / n)
     kz = k1[:, None, None]
     ky = k1[None, :, None]
     kx = k1[None, None, :]
     kk2 = kx * kx + ky * ky + kz * kz
-    kk = np.sqrt(kk2)
-    amp = kk * np.exp(-((kk / kpeak) ** 2))
+    amp = np.sqrt(kk2) * np.exp(-kk2 / (kpeak * kpeak))
     amp[0, 0, 0] = 0.0
-    a = [rng.standard_normal((n, n, n)) + 1j * rng.standard_normal((n, n, n)) for _ in range(3)]
-    kk2s = np.where(kk2 == 0, 1.0, kk2)
-    dot = (kx * a[0] + ky * a[1] + kz * a[2]) / kk2s
-    comps = [a[0] - kx * dot, a[1] - ky * dot, a[2] - kz * dot]
-    del a, dot
+    a = []
+    for _ in range(3):
+        c = rng.standard_normal((n, n, n)).astype(np.complex128)
+        c.imag = rng.standard_normal((n, n, n))
+        a.append(c)
+    kk2[0, 0, 0] = 1.0
+    dot = kx * a[0]
+    dot += ky * a[1]
+    dot += kz * a[2]
+    dot /= kk2
+    del kk2
     dx = TWO_PI / n
     # phase shifts taking grid point m*dx to the staggered positions
     shifts = [(dx, 0.5 * dx, 0.5 * dx), (0.5 * dx, dx, 0.5 * dx), (0.5 * dx, 0.5 * dx, dx)]
+    ks = (kx, ky, kz)
     out = []
     for c in range(3):
         sx, sy, sz = shifts[c]
-        ph = np.exp(1j * (kx * sx + ky * sy + kz * sz))
-        f = np.fft.ifftn((comps[c] * amp * ph).astype(dtype)).real * (n ** 3)
-        out.append(f.astype(np.float64))
-    del comps
-    e = (out[0] ** 2 + out[1] ** 2 + out[2] ** 2).mean() / 3.0
+        comp = a[c]
+        comp -= ks[c] * dot
+        comp *= amp
+        comp *= np.exp(1j * kx * sx)
+        comp *= np.exp(1j * ky * sy)
+        comp *= np.exp(1j * kz * sz)
+        a[c] = None
+        f = ifftn(comp.astype(dtype, copy=False)).real * float(n ** 3)
+        del comp
+        out.append(np.ascontiguousarray(f, dtype=np.float64))
+    del dot, a
+    e = float(np.mean(out[0] * out[0] + out[1] * out[1] + out[2] * out[2])) / 3.0
     scale = urms / math.sqrt(e)
-    U, V, W = (f * scale for f in out)
+    for f in out:
+        f *= scale
+    U, V, W = out
     return U, V, W, np.zeros((n, n, n))
 
 

@@ -79,8 +79,17 @@ def energy_spectrum(U: np.ndarray, V: np.ndarray, W: np.ndarray) -> np.ndarray:
     nbins = int(shell.max()) + 1
     e = np.zeros(nbins)
     norm = float(nx * ny * nz)
+    try:
+        import os
+
+        import scipy.fft as sfft
+
+        def rfftn(a):
+            return sfft.rfftn(a, workers=os.cpu_count() or 1)
+    except ImportError:
+        rfftn = np.fft.rfftn
     for a in (U, V, W):
-        h = np.fft.rfftn(a) / norm
+        h = rfftn(a) / norm
         e3 = 0.5 * (h.real ** 2 + h.imag ** 2) * weight[None, None, :]
         e += np.bincount(shell.ravel(), weights=e3.ravel(), minlength=nbins)
     kmax = min(nx, ny, nz) // 2

@@ -1,5 +1,7 @@
 # ccall bindings of include/lcs_b200.h (the C ABI of liblcs_b200.so).
-const LIB = joinpath(@__DIR__, "..", "..", "liblcs_b200.so")
+# LCS_B200_LIBRARY names the built library when LCSB200/ is copied beside
+# LCSCUDA/ in an LCS.jl checkout (its [sources] paths assume that place).
+const LIB = get(ENV, "LCS_B200_LIBRARY", joinpath(@__DIR__, "..", "..", "liblcs_b200.so"))
 const MAX_SPECIES = 16
 
 struct LcsSpecies

@@ -6,9 +6,9 @@ reference-owned values that pin this path are the deterministic assertions in
 its test files.  This script reads those files as text (it runs nothing from
 the reference) and writes the values, with their file:line, to
 tests/golden/known_answers.json.  The committed JSON is what the tests read;
-rerun this script only to refresh it:
+rerun this script only to refresh it, with the path of an LCS.jl checkout:
 
-    python tests/golden/make_known_answers.py /root/reference
+    python tests/golden/make_known_answers.py <path of the LCS.jl checkout>
 """
 
 import json
@@ -128,6 +128,17 @@ def main(ref):
     out["hasher"] = {"sub2ind": sub, "roundtrip_axes": [[0, 5], [0, 5], [0, 5]],
                      "expect": "encode(x) == LinearIndices((6,6,6))[x .+ 1] and decode(encode(x)) == x",
                      "source": f"test/test_utils.jl:{no}"}
+    # the package UUIDs and path sources a backend package beside LCSCUDA/ binds to
+    import tomllib
+
+    root = tomllib.load(open(os.path.join(ref, "Project.toml"), "rb"))
+    cuda = tomllib.load(open(os.path.join(ref, "LCSCUDA", "Project.toml"), "rb"))
+    out["julia_packages"] = {
+        "uuids": dict(root["deps"], LCS=root["uuid"]),
+        "root_sources": {k: v["path"] for k, v in root["sources"].items()},
+        "lcscuda_sources": {k: v["path"] for k, v in cuda["sources"].items()},
+        "source": "Project.toml [deps], [sources]; LCSCUDA/Project.toml [sources]",
+    }
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
@@ -135,4 +146,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_known_answers.py <path of the LCS.jl checkout>")
+    main(sys.argv[1])

@@ -149,7 +149,9 @@ def simulate(config, *, steps: int | None = None, quiet: bool = False, engine_cl
     resume (default with save=True: the LCS_RESUME environment variable, as
     LCSIO.init reads it; otherwise False): continue from the latest
     restart.h5.<step> in outdir, with t from stat.h5
-    (LCSIO.load_resume_state!), up to step last_step."""
+    (LCSIO.load_resume_state!).  Without `steps`, the run takes the
+    reference's last_step - step + 1 steps (its loop over state.step:last_step),
+    ending at step last_step + 1."""
     import os
 
     from . import restart
@@ -168,7 +170,9 @@ def simulate(config, *, steps: int | None = None, quiet: bool = False, engine_cl
     if resume:
         t, _ = restart.load_state(eng.lib, os.path.join(out, "stat.h5"), start)
         eng.set_state(start, t)
-    last = (rc.last_step - start) if steps is None else steps
+    # the reference loops `for _ in state.step:last_step` (src/simulate.jl:54):
+    # last_step - step + 1 steps, so a fresh run ends at step last_step + 1
+    last = (rc.last_step - start + 1) if steps is None else steps
     istat = max(1, rc.interval_stat)
     irest = rc.interval_restart if save else 0
     if save:

@@ -112,10 +112,11 @@ def test_simulate_equals_a_manual_step_loop():
     final state as one loop of timestep! + evolve! over the same init."""
     d = small_run()
     eng, logs = simulate(d, quiet=True, engine_cls=OracleEngine)
-    assert [lg["step"] for lg in logs] == [1, 2, 3]
+    # `for _ in state.step:last_step` (src/simulate.jl:54) from step 0: last_step + 1 steps
+    assert [lg["step"] for lg in logs] == [1, 2, 3, 4]
     ref = init_engine(lcfg.from_dict(d), OracleEngine)
     manual = []
-    for _ in range(3):
+    for _ in range(4):
         dt = ref.timestep()
         manual.append((dt, ref.evolve(dt)))
     for lg, (dt, ev) in zip(logs, manual):
@@ -137,7 +138,7 @@ def test_simulate_equals_a_manual_step_loop():
 def test_simulate_prints_one_line_per_step(capsys):
     eng, logs = simulate(small_run(steps=2, interval=5), engine_cls=OracleEngine)
     out = capsys.readouterr().out.strip().splitlines()
-    assert len(out) == 2 and out[0].startswith("step=1 ") and "couple1=(itr=" in out[0]
+    assert len(out) == 3 and out[0].startswith("step=1 ") and "couple1=(itr=" in out[0]
     eng.close()
 
 
@@ -149,7 +150,7 @@ def test_simulate_writes_stat_and_restart_files(tmp_path):
     from lcs_b200 import restart
     from oracle_engine import load_oracle
 
-    d = small_run(steps=6, interval=2)
+    d = small_run(steps=5, interval=2)  # steps 1..6
     d["simulate"].update({"interval_restart": 3, "num_restart_files": 1})
     for p in d["particles"]:
         p["cell"] = {"grid_ratio": 2}
@@ -182,8 +183,9 @@ def test_simulate_writes_stat_and_restart_files(tmp_path):
 
 
 def test_resume_continues_the_run(tmp_path):
-    """LCS_RESUME: a run stopped at step 3 (restart.h5.3, stat.h5) and resumed
-    to step 6 ends where an uninterrupted 6-step run ends (flow bit for bit,
+    """LCS_RESUME: a run stopped at step 4 (last_step 3; restart.h5.3, stat.h5)
+    and resumed from step 3 to step 7 (last_step 6) ends where an uninterrupted
+    run ends (flow bit for bit,
     particles by id), with the step counter and time carried over."""
     d = small_run(steps=3, interval=3)
     d["simulate"].update({"interval_restart": 3, "num_restart_files": 2})
@@ -193,7 +195,7 @@ def test_resume_continues_the_run(tmp_path):
     d6 = small_run(steps=6, interval=3)
     d6["simulate"].update({"interval_restart": 3, "num_restart_files": 2})
     resumed, rlogs = simulate(d6, quiet=True, engine_cls=OracleEngine, save=True, outdir=out, resume=True)
-    assert [lg["step"] for lg in rlogs] == [4, 5, 6]
+    assert [lg["step"] for lg in rlogs] == [4, 5, 6, 7]
     assert sorted(os.listdir(out)) == ["restart.h5.3", "restart.h5.6", "stat.h5"]
     whole, wlogs = simulate(d6, quiet=True, engine_cls=OracleEngine)
     assert rlogs[-1]["t"] == wlogs[-1]["t"] and resumed.get_state() == whole.get_state()
@@ -262,11 +264,11 @@ def test_command_line_run_and_resume(tmp_path, monkeypatch, capsys):
     with pytest.raises(ValueError, match="LCS_RESUME"):
         main([str(cfg)], engine_cls=OracleEngine)
     monkeypatch.setenv("LCS_RESUME", "1")
-    assert main([str(cfg)], engine_cls=OracleEngine) == 0  # steps 3 and 4
+    assert main([str(cfg)], engine_cls=OracleEngine) == 0  # steps 3, 4 and 5 (state.step 2 : last_step 4)
     assert sorted(os.listdir(out)) == ["config.lcs-yaml", "restart.h5.4", "stat.h5"]
     assert restart.listing(load_oracle(), str(out / "stat.h5")) == ["2", "4"]
     lines = [x for x in capsys.readouterr().out.splitlines() if x.startswith("step=")]
-    assert [x.split()[0] for x in lines] == ["step=1", "step=2", "step=3", "step=4"]
+    assert [x.split()[0] for x in lines] == ["step=1", "step=2", "step=3", "step=4", "step=5"]
 
 
 def test_backend_particle_sort_param():

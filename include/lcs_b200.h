@@ -251,6 +251,19 @@ LCS_API int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* out);
  * (W[k]-W[k-1]), periodic): its RMS and its max |div| (a diagnostic beside the
  * couple log's residual, which the reference takes over 1:n+1). */
 LCS_API int lcs_flow_divergence(lcs_handle* h, double* rms, double* maxabs);
+/* Test hook for the bounded device waits (no reference counterpart; the
+ * reference has no device-side waits).  kind 1 makes the grid barriers of the
+ * cooperative face-phase kernel of overlap sweeps wait for one arrival more
+ * than there are blocks; kind 2 makes the row-warp sweep's TMA plane barriers
+ * expect 16 bytes more than its copies deliver.  The next launch that waits
+ * then runs its wait out at the bound (about 0.1 s for a grid barrier, 2^22
+ * polls for a plane barrier; the sweep still waits, bounded, for the copies
+ * it issued before it returns), sets the handle's sticky wait error and stops
+ * the couple: the call returns LCS_ETIMEDOUT and so does every later step of
+ * the handle.  kind 0 (the default) restores normal waits; the handle stays
+ * failed and is destroyed.  No trap, no hang: the context stays usable for
+ * other handles. */
+LCS_API int lcs_debug_unreachable_waits(lcs_handle* h, int32_t kind);
 
 /* `Particles.makeindex!` (src/particles/makeindex.jl:29-67) on species s with
  * the positions of stage (1: xss, 2: xss2): cell index ci = floor(x / dxc) + 1
@@ -497,9 +510,13 @@ LCS_API const char* lcs_serve_last_error(void);
  * default stream).  It allocates nothing: its scratch is a static device array
  * of 3 * LCS_NOALLOC_MAX_PLANES doubles per GPU, held until the process exits,
  * so dims[2] may be at most LCS_NOALLOC_MAX_PLANES (larger grids get EINVAL).
- * The first call on a device looks the array up and should come before any
- * stream capture.  Every call shares the array: calls that overlap on the GPU
- * race.  Errors are reported through lcs_last_error(NULL). */
+ * Every call looks the array's device address up in the current context (a
+ * reset context gets a new one); the first call on a device loads the module
+ * and should come before any stream capture.  Every call shares the array:
+ * calls that overlap on the GPU race, so serialise them on one stream.  A NaN
+ * in U, V or W gives a NaN dt (Julia's maximum and min propagate NaN), which
+ * the caller reads with the result; the call itself returns LCS_OK.  Errors
+ * are reported through lcs_last_error(NULL). */
 #define LCS_NOALLOC_MAX_PLANES 4096
 LCS_API int lcs_flow_timestep_noalloc(const double* U, const double* V, const double* W, const int32_t dims[3],
                                       int32_t halo_size, double cfl, double dtmax, double Re, double* dt_out,

@@ -271,6 +271,10 @@ int lcs_flow_divergence(lcs_handle* h, double* rms, double* maxabs) {
   H(h);
   return h->e->flow_divergence(rms, maxabs);
 }
+int lcs_debug_unreachable_waits(lcs_handle* h, int32_t kind) {
+  H(h);
+  return h->e->debug_waits(kind);
+}
 int lcs_upload_flow_coarse(lcs_handle* h, const double* U, const double* V, const double* W, const double* P) {
   H(h);
   return h->e->upload_flow_coarse(U, V, W, P);

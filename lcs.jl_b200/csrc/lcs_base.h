@@ -82,6 +82,7 @@ struct EngineBase {
   virtual int group_create(EngineBase* const* members, int m, GroupBase** out) = 0;
   virtual const lcs_config& config() const = 0;
   virtual int flow_divergence(double* rms, double* maxabs) = 0;
+  virtual int debug_waits(int kind) = 0;
   int fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;

@@ -9,6 +9,7 @@
 // then touches whole 32-byte sectors only.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -98,6 +99,11 @@ struct Ctx {
   int wait_error;       // sticky: a bounded device wait (TMA copy, grid barrier) ran out
   unsigned int gbar_count;  // arrivals at the grid-wide barriers of a cooperative launch (0 between launches)
   double* sp_base[16];  // property block of each species: 16 FP64 properties, then the ids
+  // test hook (lcs_debug_unreachable_waits): 1 makes the grid barriers of the
+  // cooperative face kernel wait for one arrival more than there are blocks,
+  // 2 makes the sweep's TMA plane barriers expect 16 bytes more than its
+  // copies deliver; either wait then runs out at its bound.  0 in production.
+  int debug_wait;
 };
 
 // ---- stencil primitives (src/diff.jl:1-39), same evaluation order --------
@@ -111,6 +117,21 @@ template <typename T> __device__ __forceinline__ T diff2_o4_at_node(T a, T b, T 
 }
 template <typename T> __device__ __forceinline__ T sum_flux_o4(T j1a, T j1b, T j3a, T j3b) {
   return T(9.0 / 8.0) * (-j1a + j1b) - T((1.0 / 8.0) * (1.0 / 3.0)) * (-j3a + j3b);
+}
+
+// Julia's max and min of two floats (Base.max, Base.min): a NaN operand gives
+// NaN, and max(-0.0, 0.0) = 0.0, min(-0.0, 0.0) = -0.0.  C's fmax/fmin drop a
+// NaN instead, which would hide a non-finite field from maximum(abs, U) and
+// the time step built on it (src/flows/timestep.jl:48-64).
+__host__ __device__ __forceinline__ double jl_max(double a, double b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  return (a > b || (a == b && !signbit(a))) ? a : b;
+}
+__host__ __device__ __forceinline__ double jl_min(double a, double b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  return (a < b || (a == b && signbit(a))) ? a : b;
 }
 
 // mod1 onto 1..n

@@ -1259,7 +1259,7 @@ class Engine : public EngineBase {
       }
       const double Re = cfg.U0 * cfg.L0 / cfg.NU;
       const double taup = 1.0 / 18.0 * cfg.species[s].density_ratio * Re * (dmax * dmax);
-      m = std::fmin(m, std::fmin(0.5 * taup, cfg.dtmax));
+      m = jl_min(m, jl_min(0.5 * taup, cfg.dtmax));
     }
     if (cfg.n_species == 0) m = cfg.dtmax;
     return set_scalar(&dctx->dt_particles, m);
@@ -1628,6 +1628,15 @@ class Engine : public EngineBase {
     o.flatness = d4 / (d2 * d2);
     o.L = 0.0;
     o.C_epsilon = 0.0;
+    return LCS_OK;
+  }
+  // test hook: makes the bounded device waits of one kind unreachable
+  // (Ctx::debug_wait), so that the next launch that waits runs its limit out
+  int debug_waits(int kind) override {
+    if (kind < 0 || kind > 2) return fail(LCS_EINVAL, "debug wait kind must be 0, 1 or 2");
+    if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
+    LCS_TRY(launch("set_debug_wait", k_set_debug_wait, dim3(1), dim3(1), 0, dctx, kind));
+    LCS_CUDA(cudaStreamSynchronize(stream));
     return LCS_OK;
   }
   // divergence of the current velocity (diagnostic): RMS and max over n^3

@@ -180,13 +180,16 @@ __device__ __forceinline__ void hsmac_rw_body(Ctx* __restrict__ ctx, const Grid&
     const T dxi = (T)cf.dxi, dyi = (T)cf.dyi, dzi = (T)cf.dzi, dl = (T)cf.dl, om = (T)cf.omega;
     const T dti = (T)(1.0 / ctx->scal[0]);
     const int A = kAlignElems<T>;
-    const uint32_t plane_tx = (3u * VT + PT) * (uint32_t)sizeof(T);
+    // bytes of one plane's four copies (16 more under the test hook that
+    // makes the plane barriers unreachable)
+    const uint32_t plane_tx = (3u * VT + PT) * (uint32_t)sizeof(T) + (ctx->debug_wait == 2 ? 16u : 0u);
     if (tid == 0) {
       for (int q = 0; q < NS; q++) mbar_init(&bars[q], 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     int loads = 0;  // plane loads issued by this CTA: slot = index % NS, parity = (index / NS) & 1
+    int issued = 0;  // thread 0: loads issued so far (index of the next one)
     bool ok = true;
     for (int item = (int)bid; item < sc.nitems && ok; item += (int)nb) {
       int col, kb, ke;
@@ -199,6 +202,7 @@ __device__ __forceinline__ void hsmac_rw_body(Ctx* __restrict__ ctx, const Grid&
       const int load0 = loads;
       auto issue = [&](int l) {  // plane s = kb-2+l into slot (load0+l) % NS
         const int li = load0 + l, slot = li % NS;
+        issued = li + 1;
         mbar_arrive_expect_tx(&bars[slot], plane_tx);
         T* base = svel + slot * 3 * VT;
         const int cz = kb - 2 + l + h - 1;
@@ -464,9 +468,11 @@ __device__ __forceinline__ void hsmac_rw_body(Ctx* __restrict__ ctx, const Grid&
       }
     }
     if (!ok) {
-      // let the copies already issued land before the CTA's shared memory goes away
+      // let the copies already issued land before the CTA's shared memory goes
+      // away: a slot is refilled only after its previous phase was consumed, so
+      // each slot has at most one phase outstanding, that of its latest load
       if (tid == 0)
-        for (int q = 0; q < NS; q++) mbar_wait_bounded(&bars[q], 0u);
+        for (int li = max(0, issued - NS); li < issued; li++) mbar_wait_bounded(&bars[li % NS], (uint32_t)((li / NS) & 1));
       __syncthreads();
     }
   }

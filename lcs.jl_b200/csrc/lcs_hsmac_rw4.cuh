@@ -109,6 +109,7 @@ __device__ __forceinline__ void hsmac_rw4_body(Ctx* __restrict__ ctx, const Grid
     }
     __syncthreads();
     int loads = 0;
+    int issued = 0;  // thread 0: loads issued so far (index of the next one)
     bool ok = true;
     for (int item = (int)bid; item < sc.nitems && ok; item += (int)nb) {
       int col, kb, ke;
@@ -121,6 +122,7 @@ __device__ __forceinline__ void hsmac_rw4_body(Ctx* __restrict__ ctx, const Grid
       const int load0 = loads;
       auto issue = [&](int l) {
         const int li = load0 + l, slot = li % NS;
+        issued = li + 1;
         mbar_arrive_expect_tx(&bars[slot], plane_tx);
         float* base = svel + slot * 3 * VT;
         const int cz = kb - 2 + l + h - 1;
@@ -422,7 +424,7 @@ __device__ __forceinline__ void hsmac_rw4_body(Ctx* __restrict__ ctx, const Grid
     }
     if (!ok) {
       if (tid == 0)
-        for (int q = 0; q < NS; q++) mbar_wait_bounded(&bars[q], 0u);
+        for (int li = max(0, issued - NS); li < issued; li++) mbar_wait_bounded(&bars[li % NS], (uint32_t)((li / NS) & 1));
       __syncthreads();
     }
   }

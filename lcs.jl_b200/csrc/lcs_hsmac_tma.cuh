@@ -60,10 +60,18 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-// Bounded wait: true when the phase completed, false after the limit.
+// Bounded wait: true when the phase completed, false after 2^22 polls or
+// about 0.25 s (5e8 SM cycles), whichever comes first.  A try_wait may itself
+// suspend the thread for a while, so the poll count alone does not bound the
+// time.  The clock is read only once the first poll has failed.
+constexpr long long kMbarWaitCycles = 500000000;
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); it++)
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  for (int it = 0; it < (1 << 22); it++) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (clock64() - t0 > kMbarWaitCycles) break;
+  }
   return false;
 }
 
@@ -172,6 +180,7 @@ __global__ void __launch_bounds__(TmaThreads<TX, TY>::NT, TmaThreads<TX, TY>::MI
     __syncthreads();
     const int ncols = gx * gy;
     int loads = 0;  // TMA plane loads issued by this CTA: slot = index % NS, parity = (index / NS) & 1
+    int issued = 0;  // thread 0: loads issued so far (index of the next one)
     bool ok = true;
     for (int item = blockIdx.x; item < nitems && ok; item += gridDim.x) {
       const int col = item % ncols;
@@ -185,6 +194,7 @@ __global__ void __launch_bounds__(TmaThreads<TX, TY>::NT, TmaThreads<TX, TY>::MI
       const int load0 = loads;
       auto issue = [&](int l) {  // plane s = kb-2+l
         const int s = kb - 2 + l, li = load0 + l, slot = li % NS;
+        issued = li + 1;
         const bool withP = s >= kb && s <= ke;
         mbar_arrive_expect_tx(&bars[slot], vel_tx + (withP ? (uint32_t)L::P_TILE * 8u : 0u));
         double* base = svel + slot * 3 * VT;
@@ -408,7 +418,7 @@ __global__ void __launch_bounds__(TmaThreads<TX, TY>::NT, TmaThreads<TX, TY>::MI
     if (!ok) {
       // let the copies already issued land before the CTA's shared memory goes away
       if (tid == 0)
-        for (int q = 0; q < NS; q++) mbar_wait_bounded(&bars[q], 0u);
+        for (int li = max(0, issued - NS); li < issued; li++) mbar_wait_bounded(&bars[li % NS], (uint32_t)((li / NS) & 1));
       __syncthreads();
     }
   }

@@ -37,7 +37,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh /* NT/32 */) {
 
 template <int NT>
 __device__ __forceinline__ double block_max(double v, double* sh) {
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = jl_max(v, __shfl_xor_sync(0xffffffffu, v, o));
   const int w = threadIdx.x / 32, l = threadIdx.x % 32;
   __syncthreads();
   if (l == 0) sh[w] = v;
@@ -45,7 +45,7 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
   double s = 0.0;
   if (threadIdx.x == 0) {
     s = sh[0];
-    for (int q = 1; q < NT / 32; q++) s = fmax(s, sh[q]);
+    for (int q = 1; q < NT / 32; q++) s = jl_max(s, sh[q]);
   }
   return s;
 }
@@ -407,6 +407,7 @@ __device__ __forceinline__ bool grid_barrier(Ctx* ctx, unsigned int target, int*
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
+    if (ctx->debug_wait == 1) target += 1;  // test hook: an arrival that never comes
     __threadfence();  // the block's writes (ordered by the __syncthreads) before the arrival
     atomicAdd(&ctx->gbar_count, 1u);
     const long long t0 = clock64();
@@ -849,9 +850,9 @@ __global__ void __launch_bounds__(256) k_cfl_max(const Ctx* __restrict__ ctx, Gr
     const T uc = interp_o4_at_half<T>(U[c - 2], U[c - 1], U[c], U[c + 1]);
     const T vc = interp_o4_at_half<T>(V[c - 2 * g.px], V[c - g.px], V[c], V[c + g.px]);
     const T wc = interp_o4_at_half<T>(W[c - 2 * g.pz], W[c - g.pz], W[c], W[c + g.pz]);
-    mu = fmax(mu, fabs((double)uc));
-    mv = fmax(mv, fabs((double)vc));
-    mw = fmax(mw, fabs((double)wc));
+    mu = jl_max(mu, fabs((double)uc));
+    mv = jl_max(mv, fabs((double)vc));
+    mw = jl_max(mw, fabs((double)wc));
   }
   const double a = block_max<256>(mu, sh);
   const double b = block_max<256>(mv, sh);
@@ -921,12 +922,12 @@ __global__ void __launch_bounds__(256) k_flow_stat(const Ctx* __restrict__ ctx, 
     acc[5] += u;
     acc[6] += v;
     acc[7] += w;
-    acc[8] = fmax(acc[8], u);
-    acc[9] = fmax(acc[9], v);
-    acc[10] = fmax(acc[10], w);
-    acc[11] = fmin(acc[11], u);
-    acc[12] = fmin(acc[12], v);
-    acc[13] = fmin(acc[13], w);
+    acc[8] = jl_max(acc[8], u);
+    acc[9] = jl_max(acc[9], v);
+    acc[10] = jl_max(acc[10], w);
+    acc[11] = jl_min(acc[11], u);
+    acc[12] = jl_min(acc[12], v);
+    acc[13] = jl_min(acc[13], w);
   }
   for (int q = 0; q < kStatVals; q++) {
     double r;
@@ -963,7 +964,7 @@ __global__ void __launch_bounds__(256) k_div_stat(const Ctx* __restrict__ ctx, G
     const double dwdz = dzi * (-(double)W[g.at(i, j, wrap1(k - 1, nz))] + (double)W[c]);
     const double div = dudx + dvdy + dwdz;
     s2 += div * div;
-    mx = fmax(mx, fabs(div));
+    mx = jl_max(mx, fabs(div));
   }
   const double bs = block_sum<256>(s2, sh);
   const double bm = block_max<256>(mx, sh);
@@ -978,7 +979,7 @@ __global__ void __launch_bounds__(256) k_div_stat_final(const double* __restrict
   double s = 0.0, m = 0.0;
   for (int b = threadIdx.x; b < nb; b += 256) {
     s += partials[2 * b];
-    m = fmax(m, partials[2 * b + 1]);
+    m = jl_max(m, partials[2 * b + 1]);
   }
   const double bs = block_sum<256>(s, sh);
   const double bm = block_max<256>(m, sh);
@@ -995,7 +996,7 @@ __global__ void __launch_bounds__(256) k_flow_stat_final(const double* __restric
     double v = q < 8 ? 0.0 : (q < 11 ? -INFINITY : INFINITY);
     for (int b = threadIdx.x; b < nb; b += 256) {
       const double x = partials[kStatVals * b + q];
-      v = q < 8 ? v + x : (q < 11 ? fmax(v, x) : fmin(v, x));
+      v = q < 8 ? v + x : (q < 11 ? jl_max(v, x) : jl_min(v, x));
     }
     const double r = q < 8 ? block_sum<256>(v, sh) : (q < 11 ? block_max<256>(v, sh) : -block_max<256>(-v, sh));
     if (threadIdx.x == 0) out[q] = r;
@@ -1015,17 +1016,17 @@ __global__ void __launch_bounds__(256) k_cfl_finalize(Ctx* ctx, const double* __
   double m[3];
   for (int a = 0; a < 3; a++) {
     double v = 0.0;
-    for (int q = threadIdx.x; q < nb; q += 256) v = fmax(v, partials[3 * q + a]);
+    for (int q = threadIdx.x; q < nb; q += 256) v = jl_max(v, partials[3 * q + a]);
     m[a] = block_max<256>(v, sh);
   }
   if (threadIdx.x == 0) {
     const double umax = m[0] + 1e-10, vmax = m[1] + 1e-10, wmax = m[2] + 1e-10;
     double d = c.dtmax;
-    d = fmin(d, c.cfl * c.dx / umax);
-    d = fmin(d, c.cfl * c.dy / vmax);
-    d = fmin(d, c.cfl * c.dz / wmax);
-    d = fmin(d, 0.5 * ((c.dx / 2.0) * (c.dx / 2.0)) / (1.0 / c.Re));
-    if (!flow_only && c.with_particles) d = fmin(d, ctx->dt_particles);
+    d = jl_min(d, c.cfl * c.dx / umax);
+    d = jl_min(d, c.cfl * c.dy / vmax);
+    d = jl_min(d, c.cfl * c.dz / wmax);
+    d = jl_min(d, 0.5 * ((c.dx / 2.0) * (c.dx / 2.0)) / (1.0 / c.Re));
+    if (!flow_only && c.with_particles) d = jl_min(d, ctx->dt_particles);
     if (!(d > 0.0) || !isfinite(d)) ctx->nonfinite = 1;
     if (!flow_only) {
       ctx->dt = d;
@@ -1213,7 +1214,7 @@ __global__ void k_rcf_spectrum(const double* __restrict__ hat, int kmin, int kma
           }
         }
     const double en = e / 2.0;
-    r_of_shell[k0 - kmin] = sqrt(en0[k0 - kmin] / fmax(en, 1e-8)) - 1.0;
+    r_of_shell[k0 - kmin] = sqrt(en0[k0 - kmin] / jl_max(en, 1e-8)) - 1.0;
   }
   for (int a = 0; a < 3; a++)
     for (int kz = -kmax; kz <= kmax; kz++)
@@ -1489,7 +1490,7 @@ __global__ void k_particles_init_velocity(const Ctx* __restrict__ ctx, Grid g, i
 __global__ void __launch_bounds__(256) k_max_reduce(const double* __restrict__ a, int64_t n, double* __restrict__ out) {
   __shared__ double sh[8];
   double v = 0.0;
-  for (int64_t q = threadIdx.x; q < n; q += 256) v = fmax(v, a[q]);
+  for (int64_t q = threadIdx.x; q < n; q += 256) v = jl_max(v, a[q]);
   const double m = block_max<256>(v, sh);
   if (threadIdx.x == 0) *out = m;
 }
@@ -1571,6 +1572,7 @@ __global__ void k_convert_out(double* __restrict__ dst, const T* __restrict__ sr
 // --------------------------------------------------------------------------
 __global__ void k_set_stage_dt(Ctx* ctx, int stage) { ctx->scal[0] = stage == 1 ? 0.5 * ctx->dt : ctx->dt; }
 __global__ void k_set_scalar(double* dst, double v) { *dst = v; }
+__global__ void k_set_debug_wait(Ctx* ctx, int kind) { ctx->debug_wait = kind; }
 __global__ void k_set_species_base(Ctx* ctx, int s, double* base) { ctx->sp_base[s] = base; }
 __global__ void k_step_begin(Ctx* ctx) {
   ctx->cur.p = __longlong_as_double(0x7ff8000000000000LL);

@@ -14,7 +14,6 @@
 
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/lcs_b200.h"
 
@@ -25,16 +24,11 @@ void set_global_error_message(const char* msg);  // lcs_api.cu: lcs_last_error(N
 namespace {
 
 constexpr int kMaxPlanes = LCS_NOALLOC_MAX_PLANES;
-constexpr int kMaxDevices = 64;
 constexpr double kTwoPi = 2.0 * 3.14159265358979323846;
 
 // Per-plane partial maxima of |U|, |V|, |W| interpolated to the cell centre:
 // [component][plane].  Shared by every call on a device.
 static __device__ __align__(256) double g_cfl_scratch[3 * kMaxPlanes];
-
-std::mutex g_setup_mutex;
-double* g_scratch_dev[kMaxDevices];  // device address of g_cfl_scratch, per device
-bool g_scratch_ready[kMaxDevices];
 
 int fail(int code, const char* msg) {
   lcs::set_global_error_message(msg);
@@ -56,6 +50,18 @@ __device__ __forceinline__ long long at(const Layout& L, int i, int j, int k) {
 __device__ __forceinline__ double o4(double a, double b, double c, double d) {
   return (1.0 / 16.0) * (-a + 9.0 * b + 9.0 * c - d);
 }
+// Julia's max/min of floats: a NaN operand gives NaN (fmax/fmin would drop
+// it), so a non-finite U, V or W gives a NaN dt as maximum(abs, U) does.
+__device__ __forceinline__ double jl_max(double a, double b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  return (a > b || (a == b && !signbit(a))) ? a : b;
+}
+__device__ __forceinline__ double jl_min(double a, double b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  return (a < b || (a == b && signbit(a))) ? a : b;
+}
 
 // One block per z-plane: the plane's maxima of |uc|, |vc|, |wc|, the o4
 // cell-centre interpolations of flows/timestep.jl:35-45.  The interior is
@@ -75,20 +81,20 @@ __global__ void __launch_bounds__(256) k_cfl_planes(const double* __restrict__ U
                          V[at(L, i, wrap1(j + 1, ny), k)]);
     const double wc = o4(W[at(L, i, j, wrap1(k - 2, nz))], W[at(L, i, j, wrap1(k - 1, nz))], W[at(L, i, j, k)],
                          W[at(L, i, j, wrap1(k + 1, nz))]);
-    mu = fmax(mu, fabs(uc));
-    mv = fmax(mv, fabs(vc));
-    mw = fmax(mw, fabs(wc));
+    mu = jl_max(mu, fabs(uc));
+    mv = jl_max(mv, fabs(vc));
+    mw = jl_max(mw, fabs(wc));
   }
   double m[3] = {mu, mv, mw};
   for (int c = 0; c < 3; c++) {
     double v = m[c];
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = jl_max(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (threadIdx.x % 32 == 0) sh[c][threadIdx.x / 32] = v;
   }
   __syncthreads();
   if (threadIdx.x < 3) {
     double v = sh[threadIdx.x][0];
-    for (int w = 1; w < 8; w++) v = fmax(v, sh[threadIdx.x][w]);
+    for (int w = 1; w < 8; w++) v = jl_max(v, sh[threadIdx.x][w]);
     scratch[threadIdx.x * kMaxPlanes + blockIdx.x] = v;  // every slot of this call is rewritten
   }
 }
@@ -102,8 +108,8 @@ __global__ void __launch_bounds__(256) k_cfl_final(const double* scratch, int nz
   __shared__ double sh[3][8];
   for (int c = 0; c < 3; c++) {
     double v = 0.0;
-    for (int k = threadIdx.x; k < nz; k += blockDim.x) v = fmax(v, scratch[c * kMaxPlanes + k]);
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) v = jl_max(v, scratch[c * kMaxPlanes + k]);
+    for (int o = 16; o > 0; o >>= 1) v = jl_max(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (threadIdx.x % 32 == 0) sh[c][threadIdx.x / 32] = v;
   }
   __syncthreads();
@@ -111,38 +117,39 @@ __global__ void __launch_bounds__(256) k_cfl_final(const double* scratch, int nz
     double m[3];
     for (int c = 0; c < 3; c++) {
       m[c] = sh[c][0];
-      for (int w = 1; w < 8; w++) m[c] = fmax(m[c], sh[c][w]);
+      for (int w = 1; w < 8; w++) m[c] = jl_max(m[c], sh[c][w]);
       m[c] = m[c] + 1e-10;
     }
     double d = a.dtmax;
-    d = fmin(d, a.cfl * a.dx / m[0]);
-    d = fmin(d, a.cfl * a.dy / m[1]);
-    d = fmin(d, a.cfl * a.dz / m[2]);
-    d = fmin(d, 0.5 * ((a.dx / 2.0) * (a.dx / 2.0)) / (1.0 / a.Re));
+    d = jl_min(d, a.cfl * a.dx / m[0]);
+    d = jl_min(d, a.cfl * a.dy / m[1]);
+    d = jl_min(d, a.cfl * a.dz / m[2]);
+    d = jl_min(d, 0.5 * ((a.dx / 2.0) * (a.dx / 2.0)) / (1.0 / a.Re));
     *dt_out = d;
   }
 }
 
-// Device address of the scratch array on the current device, looked up once
-// per device (host code only sees a host-side stand-in for the symbol).
+// Device address of the scratch array in the current device's context.  Host
+// code only sees a host-side stand-in for the symbol, so the address is looked
+// up with cudaGetSymbolAddress (which allocates nothing) on every call: a
+// context that the caller reset or destroyed and created again (CUDA.jl's
+// device_reset!, cudaDeviceReset) loads the module again at another address,
+// and an address kept from before would point into freed memory.  The first
+// call on a device loads the module, so it should come before any stream
+// capture.
 int scratch_for_current_device(double** out) {
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
     cudaGetLastError();
     return fail(LCS_ECUDA, "lcs_flow_timestep_noalloc: no current CUDA device");
   }
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ready[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_cfl_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      cudaGetLastError();
-      return fail(LCS_ECUDA, "lcs_flow_timestep_noalloc: cudaGetSymbolAddress of the scratch array failed");
-    }
-    g_scratch_dev[dev] = (double*)p;
-    g_scratch_ready[dev] = true;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_cfl_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    cudaGetLastError();
+    return fail(LCS_ECUDA, "lcs_flow_timestep_noalloc: cudaGetSymbolAddress of the scratch array failed");
   }
-  *out = g_scratch_dev[dev];
+  *out = (double*)p;
   return LCS_OK;
 }
 

@@ -36,8 +36,8 @@ __global__ void __launch_bounds__(256) k_psummary(const double* X, const double*
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
       const double a = A[q][i];
       s += a;
-      mx = fmax(mx, a);
-      mn = fmin(mn, a);
+      mx = jl_max(mx, a);
+      mn = jl_min(mn, a);
     }
     const double bs = block_sum<256>(s, sh);
     const double bmx = block_max<256>(mx, sh);
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(256) k_psummary_final(const double* __restrict
     double v = kind == 0 ? 0.0 : (kind == 1 ? -INFINITY : INFINITY);
     for (int b = threadIdx.x; b < nb; b += 256) {
       const double x = partials[kPSumVals * b + q];
-      v = kind == 0 ? v + x : (kind == 1 ? fmax(v, x) : fmin(v, x));
+      v = kind == 0 ? v + x : (kind == 1 ? jl_max(v, x) : jl_min(v, x));
     }
     const double r = kind == 0 ? block_sum<256>(v, sh) : (kind == 1 ? block_max<256>(v, sh) : -block_max<256>(-v, sh));
     if (threadIdx.x == 0) out[q] = r;

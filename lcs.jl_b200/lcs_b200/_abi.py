@@ -255,6 +255,7 @@ PROTOTYPES = {
     "lcs_get_config": (C.c_int, [_P, C.POINTER(Config)]),
     "lcs_measure_fp64_peak": (C.c_int, [C.c_int32, _D]),
     "lcs_flow_divergence": (C.c_int, [_P, _D, _D]),
+    "lcs_debug_unreachable_waits": (C.c_int, [_P, C.c_int32]),
     "lcs_restart_save": (C.c_int, [_P, C.c_char_p]),
     "lcs_restart_load": (C.c_int, [_P, C.c_char_p]),
     "lcs_restart_load_coarse": (C.c_int, [_P, C.c_char_p]),

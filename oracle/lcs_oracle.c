@@ -100,6 +100,19 @@ static inline size_t IN(const grid_t* g, int i, int j, int k) {
 }
 
 static double spacing(const grid_t* g, int a) { return DOMAIN_LENGTH / g->n[a]; } /* src/config.jl:89 */
+/* Base.max / Base.min of Julia on floats: NaN if either operand is NaN, and
+ * max(-0.0, 0.0) = 0.0, min(-0.0, 0.0) = -0.0 (C's fmax/fmin drop a NaN).
+ * `maximum`, `minimum` and `min(cands...)` reduce with them. */
+static inline double jl_max(double a, double b) {
+  if (isnan(a)) return a;
+  if (isnan(b)) return b;
+  return (a > b || (a == b && !signbit(a))) ? a : b;
+}
+static inline double jl_min(double a, double b) {
+  if (isnan(a)) return a;
+  if (isnan(b)) return b;
+  return (a < b || (a == b && signbit(a))) ? a : b;
+}
 static double Re_of(const lcs_config* c) { return c->U0 * c->L0 / c->NU; }      /* flows/config.jl:18 */
 
 /* ---- stencil primitives (src/diff.jl:1-39) ----------------------------- */
@@ -421,7 +434,8 @@ static double flow_timestep(lcs_handle* h) {
       for (int j = 1; j <= g->n[1]; j++)
         for (int i = 1; i <= g->n[0]; i++) {
           double v = fabs(h->Ui[a][IX(g, i, j, k)]);
-          if (first || v > mx[a]) { mx[a] = v; first = 0; }
+          mx[a] = first ? v : jl_max(mx[a], v);  /* maximum(abs, ...): NaN propagates */
+          first = 0;
         }
     mx[a] = mx[a] + 1e-10;
   }
@@ -430,7 +444,7 @@ static double flow_timestep(lcs_handle* h) {
   double cands[5] = {c->dtmax, c->cfl * dx / mx[0], c->cfl * dy / mx[1], c->cfl * dz / mx[2],
                      0.5 * ((dx / 2.0) * (dx / 2.0)) / (1.0 / Re)};
   double m = cands[0];
-  for (int q = 1; q < 5; q++) m = fmin(m, cands[q]);
+  for (int q = 1; q < 5; q++) m = jl_min(m, cands[q]);
   return m;
 }
 
@@ -444,9 +458,9 @@ static double particles_timestep(lcs_handle* h) { /* src/particles/timestep.jl:6
   double m = INFINITY;
   for (int s = 0; s < c->n_species; s++) {
     double dmax = 0.0;
-    for (int64_t p = 0; p < h->sp[s].n; p++) dmax = fmax(dmax, h->sp[s].p[LCS_PROP_DIAM][p]);
+    for (int64_t p = 0; p < h->sp[s].n; p++) dmax = jl_max(dmax, h->sp[s].p[LCS_PROP_DIAM][p]);
     double tp = taup(c, &c->species[s], dmax);
-    m = fmin(m, fmin(0.5 * tp, c->dtmax));
+    m = jl_min(m, jl_min(0.5 * tp, c->dtmax));
   }
   return m;
 }
@@ -645,7 +659,7 @@ static double forcing_rcf(lcs_handle* h, double dt, double* e10_out) {
     double lo = (k0 - 0.5) * (k0 - 0.5), hi = (k0 + 0.5) * (k0 + 0.5);
     double en = enespe_cropped(hat, kmax, k0, norm);
     double en0 = enespe0(k0, e10);
-    double r = sqrt(en0 / fmax(en, 1e-8)) - 1.0;
+    double r = sqrt(en0 / jl_max(en, 1e-8)) - 1.0;
     for (int kz = -kmax; kz <= kmax; kz++)
       for (int ky = -kmax; ky <= kmax; ky++)
         for (int kx = 0; kx <= kmax; kx++) {
@@ -922,6 +936,12 @@ void lcs_destroy(lcs_handle* h) {
 
 const char* lcs_last_error(const lcs_handle* h) { return h ? h->err : g_err; }
 
+/* The oracle has no device waits: the test hook only checks its argument. */
+int lcs_debug_unreachable_waits(lcs_handle* h, int32_t kind) {
+  if (!h) return LCS_EINVAL;
+  if (kind < 0 || kind > 2) return fail(h, LCS_EINVAL, "debug wait kind must be 0, 1 or 2");
+  return LCS_OK;
+}
 static int wrapi(int i, int n);
 int lcs_flow_divergence(lcs_handle* h, double* rms, double* maxabs) {
   if (!h) return LCS_EINVAL;
@@ -937,7 +957,7 @@ int lcs_flow_divergence(lcs_handle* h, double* rms, double* maxabs) {
         const double dwdz = dzi * (-h->W[IX(g, i, j, wrapi(k - 1, nz))] + h->W[IX(g, i, j, k)]);
         const double div = dudx + dvdy + dwdz;
         s2 += div * div;
-        mx = fmax(mx, fabs(div));
+        mx = jl_max(mx, fabs(div));
       }
   if (rms) *rms = sqrt(s2 / ((double)nx * ny * nz));
   if (maxabs) *maxabs = mx;
@@ -1172,7 +1192,7 @@ int lcs_particles_timestep(lcs_handle* h, double* dt) {
 int lcs_timestep(lcs_handle* h, double* dt) {
   if (!h || !dt) return LCS_EINVAL;
   double f = flow_timestep(h);
-  if (h->cfg.mode == LCS_MODE_FLOW_PARTICLE) f = fmin(f, particles_timestep(h));
+  if (h->cfg.mode == LCS_MODE_FLOW_PARTICLE) f = jl_min(f, particles_timestep(h));
   if (!isfinite(f) || f <= 0) return fail(h, LCS_ENONFINITE, "dt is not finite/positive: %g", f);
   *dt = f;
   return LCS_OK;
@@ -1283,8 +1303,8 @@ int lcs_flow_stat(lcs_handle* h, lcs_flow_stats* o) {
         const double d2 = dudx * dudx;
         sd2 += d2; sd3 += d2 * dudx; sd4 += d2 * d2;
         su += u; sv += v; sw += w;
-        mxu = fmax(mxu, u); mxv = fmax(mxv, v); mxw = fmax(mxw, w);
-        mnu = fmin(mnu, u); mnv = fmin(mnv, v); mnw = fmin(mnw, w);
+        mxu = jl_max(mxu, u); mxv = jl_max(mxv, v); mxw = jl_max(mxw, w);
+        mnu = jl_min(mnu, u); mnv = jl_min(mnv, v); mnw = jl_min(mnw, w);
       }
 #undef A
   const double N = (double)nx * ny * nz;
@@ -1506,8 +1526,8 @@ int lcs_particles_stat(lcs_handle* h, int32_t s, const lcs_particle_stat_config*
     double sum = 0.0, mx = -INFINITY, mn = INFINITY;
     for (int64_t i = 0; i < n; i++) {
       sum += a[i];
-      mx = fmax(mx, a[i]);
-      mn = fmin(mn, a[i]);
+      mx = jl_max(mx, a[i]);
+      mn = jl_min(mn, a[i]);
     }
     S[q]->mean = sum / (double)n;
     S[q]->max = mx;
@@ -1800,16 +1820,16 @@ int lcs_flow_timestep_noalloc(const double* U, const double* V, const double* W,
                                       V[IX(&g, i, j, k)], V[IX(&g, i, wrap1(j + 1, ny), k)]);
         double wc = interp_o4_at_half(W[IX(&g, i, j, wrap1(k - 2, nz))], W[IX(&g, i, j, wrap1(k - 1, nz))],
                                       W[IX(&g, i, j, k)], W[IX(&g, i, j, wrap1(k + 1, nz))]);
-        mx[0] = fmax(mx[0], fabs(uc));
-        mx[1] = fmax(mx[1], fabs(vc));
-        mx[2] = fmax(mx[2], fabs(wc));
+        mx[0] = jl_max(mx[0], fabs(uc));
+        mx[1] = jl_max(mx[1], fabs(vc));
+        mx[2] = jl_max(mx[2], fabs(wc));
       }
   double dx = DOMAIN_LENGTH / g.n[0], dy = DOMAIN_LENGTH / g.n[1], dz = DOMAIN_LENGTH / g.n[2];
   double d = dtmax;
-  d = fmin(d, cfl * dx / (mx[0] + 1e-10));
-  d = fmin(d, cfl * dy / (mx[1] + 1e-10));
-  d = fmin(d, cfl * dz / (mx[2] + 1e-10));
-  d = fmin(d, 0.5 * ((dx / 2.0) * (dx / 2.0)) / (1.0 / Re));
+  d = jl_min(d, cfl * dx / (mx[0] + 1e-10));
+  d = jl_min(d, cfl * dy / (mx[1] + 1e-10));
+  d = jl_min(d, cfl * dz / (mx[2] + 1e-10));
+  d = jl_min(d, 0.5 * ((dx / 2.0) * (dx / 2.0)) / (1.0 / Re));
   *dt_out = d;
   return LCS_OK;
 }

@@ -72,3 +72,23 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
                                        0.3, 1.0, 100.0, C.c_void_p(out.data_ptr()), None)
     assert rc == _abi.EINVAL
     assert b"z-planes" in lib.lcs_last_error(None)
+
+
+def test_noalloc_nan_cell_gives_nan_dt():
+    """Julia's maximum(abs, U) propagates a NaN: so does the entry point, and
+    the handle-based time step agrees."""
+    torch = pytest.importorskip("torch")
+    lib = _abi.load_library()
+    dims, h = (16, 16, 16), 3
+    rng = np.random.default_rng(7)
+    shape = (dims[2], dims[1], dims[0])
+    U, V, W = (rng.standard_normal(shape) for _ in range(3))
+    W[4, 5, 6] = np.nan
+    dev = [torch.from_numpy(haloed(a, h, 0.0)).to("cuda") for a in (U, V, W)]
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rc = lib.lcs_flow_timestep_noalloc(*(C.c_void_p(t.data_ptr()) for t in dev), (C.c_int32 * 3)(*dims), h, 0.3,
+                                       1.0, 100.0, C.c_void_p(out.data_ptr()), None)
+    assert rc == 0, lib.lcs_last_error(None)
+    torch.cuda.synchronize()
+    assert np.isnan(float(out.item()))

@@ -78,6 +78,8 @@ def check_assignment(rc, g, o, fo, parts_o):
     motion! and the cell index are bit-exact."""
     for e in (g, o):
         e.upload_flow(*fo)
+        # motion! reads the halo that evolve!'s FullHalo synchalo! fills first (src/evolve.jl:74-81)
+        e.synchalo([F.FIELD_U, F.FIELD_V, F.FIELD_W], 3, True)
         for s, po in enumerate(parts_o):
             e.upload_particles(s, po["diam"], po["x"], po["y"], po["z"], po["u"], po["v"], po["w"], ids=po["ids"])
     for s in range(len(parts_o)):

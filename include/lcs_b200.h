@@ -396,10 +396,12 @@ LCS_API int lcs_step_finish(lcs_handle* h, lcs_log* logs);
 LCS_API int lcs_device_bytes(lcs_handle* h, int64_t* bytes);
 /* Launch shapes of a handle, set from outside (no reference counterpart; the
  * batch's autotuner and the server use it): rw_rows = tile rows of the
- * HSMAC sweep (13, 8 or 5; 0 keeps the current), zchunk = planes per z chunk
+ * HSMAC sweep (13, 8 or 5, or 29 in FP32: two rows a warp; 0 keeps the
+ * current), zchunk = planes per z chunk
  * of a sweep (0: the built-in cost model), share = the part of the GPU the
  * handle's launches are sized for when several handles run at once (0, 1].
- * Results do not depend on these; the step graphs are captured again. */
+ * FP64 fields do not depend on these (the residual's partial sums are grouped
+ * differently); the step graphs are captured again. */
 LCS_API int lcs_set_tuning(lcs_handle* h, int32_t rw_rows, int32_t zchunk, double share);
 
 /* ---- batching form (no reference counterpart) ---------------------------

@@ -72,6 +72,7 @@ struct CoupleState {
   int sweeps;   // sweeps executed
   int done;     // exit criterion met
   int cont;     // WHILE-loop condition value (itr < itrmax && !done)
+  int groups;   // iterations of the graph's WHILE loop so far (bounds it)
   double div;   // last residual
   double sum;   // last sum of div^2
 };

@@ -375,11 +375,12 @@ class Engine : public EngineBase {
     encode_fn = encode;
     if (use_rw) {
       // row-warp sweep tile rows: LCS_B200_RW=13 (default: one CTA of 16 warps
-      // per SM, fastest in both precisions) | 8 | 5
+      // per SM, a row per warp, fastest at 512^3 in both precisions) | 8 | 5 |
+      // 29 (FP32 only: 16 warps of two rows each, faster at 256^3)
       rw_variant = 0;
       if (const char* v = std::getenv("LCS_B200_RW")) {
         const std::string t(v);
-        rw_variant = t == "8" ? 1 : t == "5" ? 2 : 0;
+        rw_variant = t == "8" ? 1 : t == "5" ? 2 : (t == "29" && std::is_same<T, float>::value) ? 3 : 0;
       }
       const char* q4 = std::getenv("LCS_B200_RW4");
       use_rw4 = std::is_same<T, float>::value && q4 && std::string(q4) == "1";
@@ -398,8 +399,15 @@ class Engine : public EngineBase {
               rw_threads = RwLayout<T, 8, 3>::NT; break;
       case 2: RTY = 5; rw_smem = RwLayout<T, 5, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 5, 3>;
               rw_threads = RwLayout<T, 5, 3>::NT; break;
-      default: RTY = 13; rw_smem = RwLayout<T, 13, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 13, 3>;
-               rw_threads = RwLayout<T, 13, 3>::NT; break;
+      case 3:
+        if constexpr (std::is_same<T, float>::value) {
+          RTY = 29; rw_smem = RwLayout<T, 29, 3, 2>::total; rw_fn = (const void*)k_hsmac_rw<T, 29, 3, 2>;
+          rw_threads = RwLayout<T, 29, 3, 2>::NT;
+          break;
+        }
+        return fail(LCS_EINVAL, "29-row sweep tiles are FP32 only");
+      default: RTY = 13; rw_smem = RwLayout<T, 13, kRwRing<T>>::total; rw_fn = (const void*)k_hsmac_rw<T, 13, kRwRing<T>>;
+               rw_threads = RwLayout<T, 13, kRwRing<T>>::NT; break;
     }
     const CUtensorMapDataType dtype =
         std::is_same<T, double>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -422,7 +430,10 @@ class Engine : public EngineBase {
     LCS_CUDA(cudaFuncSetAttribute(rw_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
     const void* rw_group_fn = rw_variant == 1   ? (const void*)k_hsmac_rw_group<T, 8, 3>
                               : rw_variant == 2 ? (const void*)k_hsmac_rw_group<T, 5, 3>
-                                                : (const void*)k_hsmac_rw_group<T, 13, 3>;
+                                                : (const void*)k_hsmac_rw_group<T, 13, kRwRing<T>>;
+    if constexpr (std::is_same<T, float>::value) {
+      if (rw_variant == 3) rw_group_fn = (const void*)k_hsmac_rw_group<T, 29, 3, 2>;
+    }
     LCS_CUDA(cudaFuncSetAttribute(rw_group_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
     LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rw_ctas_per_sm, rw_fn, rw_threads, rw_smem));
     if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the row-warp sweep does not fit on an SM");
@@ -741,12 +752,17 @@ class Engine : public EngineBase {
     if (nblocks) *nblocks = nitems;
     if (grp) return fused_rw_group(set, D, out, gb, xo, gx, gy, sc, finalize, group_end);
     const dim3 grid(nitems), block(rw_threads);
+    if constexpr (std::is_same<T, float>::value) {
+      if (rw_variant == 3)
+        return launch("hsmac_rw", k_hsmac_rw<T, 29, 3, 2>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P, D, out, gb,
+                      xo, gx, gy, sc, hc, part, finalize, group_end);
+    }
     switch (rw_variant) {
       case 1: return launch("hsmac_rw", k_hsmac_rw<T, 8, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P, D,
                             out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
       case 2: return launch("hsmac_rw", k_hsmac_rw<T, 5, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P, D,
                             out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
-      default: return launch("hsmac_rw", k_hsmac_rw<T, 13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P,
+      default: return launch("hsmac_rw", k_hsmac_rw<T, 13, kRwRing<T>>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P,
                              D, out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
     }
   }
@@ -814,12 +830,18 @@ class Engine : public EngineBase {
       }
       const dim3 grid(sc.nitems, mc), block(rw_threads);
       int rc2;
+      if constexpr (std::is_same<T, float>::value)
+        if (rw_variant == 3) {
+          LCS_TRY(launch("hsmac_rw", k_hsmac_rw_group<T, 29, 3, 2>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
+                         gx, gy, sc, hc, finalize, group_end));
+          continue;
+        }
       switch (rw_variant) {
         case 1: rc2 = launch("hsmac_rw", k_hsmac_rw_group<T, 8, 3>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
                              gx, gy, sc, hc, finalize, group_end); break;
         case 2: rc2 = launch("hsmac_rw", k_hsmac_rw_group<T, 5, 3>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
                              gx, gy, sc, hc, finalize, group_end); break;
-        default: rc2 = launch("hsmac_rw", k_hsmac_rw_group<T, 13, 3>, grid, block, rw_smem, ga, g, set, D, out, gb,
+        default: rc2 = launch("hsmac_rw", k_hsmac_rw_group<T, 13, kRwRing<T>>, grid, block, rw_smem, ga, g, set, D, out, gb,
                               xo, gx, gy, sc, hc, finalize, group_end);
       }
       LCS_TRY(rc2);
@@ -978,6 +1000,9 @@ class Engine : public EngineBase {
     return LCS_OK;
   }
   int sweeps_per_group() const { return cfg.time_blocking ? 3 : 1; }
+  // iterations of a couple's loop: at most ceil(itrmax / sweeps per group),
+  // plus a margin (the device loop and the host loop use the same bound)
+  int max_loop_groups() const { return cfg.itrmax / sweeps_per_group() + 2; }
 
   int read_ctx() {
     LCS_TRY(copy(hctx, dctx, sizeof(Ctx), cudaMemcpyDeviceToHost));
@@ -996,7 +1021,7 @@ class Engine : public EngineBase {
     const int spg = sweeps_per_group();
     // the device advances itr by one per sweep until it exits; the group
     // count is bounded so the host loop ends even if that ever failed
-    const int max_groups = cfg.itrmax / spg + 2;
+    const int max_groups = max_loop_groups();
     for (int grp = 0; itr < cfg.itrmax; grp++) {
       if (grp >= max_groups) return fail(LCS_ETIMEDOUT, "HSMAC loop did not advance");
       LCS_TRY(couple_group(set));
@@ -1110,7 +1135,7 @@ class Engine : public EngineBase {
     stream = side;
     int rc2 = couple_group(set);
     if (rc2 == LCS_OK)
-      rc2 = launch("couple_continue", k_couple_continue, dim3(1), dim3(1), 0, (const Ctx*)dctx, handle);
+      rc2 = launch("couple_continue", k_couple_continue, dim3(1), dim3(1), 0, dctx, handle, max_loop_groups());
     stream = main;
     cudaGraph_t body_out;
     cudaError_t e = cudaStreamEndCapture(side, &body_out);
@@ -1371,12 +1396,14 @@ class Engine : public EngineBase {
   // The step graphs are captured again with the new shapes.
   int set_tuning(int rw_rows, int zchunk, double share) override {
     if (async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on this handle");
-    if (rw_rows != 0 && rw_rows != 13 && rw_rows != 8 && rw_rows != 5) return fail(LCS_EINVAL, "rw_rows must be 0, 13, 8 or 5");
+    if (rw_rows != 0 && rw_rows != 13 && rw_rows != 8 && rw_rows != 5 && rw_rows != 29)
+      return fail(LCS_EINVAL, "rw_rows must be 0, 13, 8, 5 or 29 (FP32)");
+    if (rw_rows == 29 && !std::is_same<T, float>::value) return fail(LCS_EINVAL, "29-row sweep tiles are FP32 only");
     if (zchunk < 0) return fail(LCS_EINVAL, "zchunk < 0");
     if (!(share > 0.0 && share <= 1.0)) return fail(LCS_EINVAL, "share must be in (0, 1]");
     LCS_CUDA(cudaStreamSynchronize(stream));
     if (rw_rows != 0 && use_rw) {
-      rw_variant = rw_rows == 8 ? 1 : rw_rows == 5 ? 2 : 0;
+      rw_variant = rw_rows == 8 ? 1 : rw_rows == 5 ? 2 : rw_rows == 29 ? 3 : 0;
       LCS_TRY(init_rw_maps());
     }
     zchunk_force = zchunk;
@@ -2109,7 +2136,7 @@ struct EngineGroup : GroupBase {
       rc2 = L->couple_group(set);
       if (rc2 == LCS_OK)
         rc2 = L->launch("couple_continue", k_group_continue<T>, dim3(1), dim3(1), 0, L->grp_ptrs, (int)mem.size(),
-                        handle);
+                        handle, L->max_loop_groups());
       L->grp = nullptr;
       L->stream = s;
       if (rc2 != LCS_OK) rc2 = member_fail(L, rc2);

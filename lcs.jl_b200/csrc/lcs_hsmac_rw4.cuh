@@ -434,7 +434,10 @@ __device__ __forceinline__ void hsmac_rw4_body(Ctx* __restrict__ ctx, const Grid
     if (skip || ctx->wait_error) {
       if (tid == 0) {
         ctx->ticket = 0;
-        if (ctx->wait_error) ctx->cs.done = 1;
+        if (ctx->wait_error) {  // stop the couple: no more sweeps, and the graph's loop ends
+          ctx->cs.done = 1;
+          ctx->cs.cont = 0;
+        }
       }
       return;
     }

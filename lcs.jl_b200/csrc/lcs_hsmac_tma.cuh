@@ -431,7 +431,10 @@ __global__ void __launch_bounds__(TmaThreads<TX, TY>::NT, TmaThreads<TX, TY>::MI
     if (skip || ctx->wait_error) {
       if (tid == 0) {
         ctx->ticket = 0;
-        if (ctx->wait_error) ctx->cs.done = 1;
+        if (ctx->wait_error) {  // stop the couple: no more sweeps, and the graph's loop ends
+          ctx->cs.done = 1;
+          ctx->cs.cont = 0;
+        }
       }
       return;
     }

@@ -547,6 +547,7 @@ __device__ __forceinline__ void hsmac_faces_body(Ctx* __restrict__ ctx, const Gr
       } else {
         ctx->wait_error = 1;
         ctx->cs.done = 1;
+        ctx->cs.cont = 0;
       }
     }
   }
@@ -801,6 +802,7 @@ __global__ void k_couple_reset(Ctx* ctx, int itrmax) {
   ctx->cs.div = 0.0;
   ctx->cs.sum = 0.0;
   ctx->cs.cont = itrmax > 0 ? 1 : 0;
+  ctx->cs.groups = 0;
   ctx->ticket = 0;
 }
 
@@ -818,15 +820,25 @@ __global__ void k_couple_log(Ctx* ctx, int stage) {
 }
 
 // WHILE-node condition of the device-resident couple loop.
-__global__ void k_couple_continue(const Ctx* ctx, cudaGraphConditionalHandle handle) {
-  cudaGraphSetConditional(handle, ctx->cs.cont ? 1u : 0u);
+// The loop goes on while the exit test says so, no sweep has stopped the
+// couple (a failed bounded wait, a non-finite residual) and fewer than
+// max_groups iterations have run (the reference's loop runs at most
+// ceil(itrmax / sweeps per group) of them; the bound holds the loop even if a
+// kernel failed before its exit test).
+__device__ __forceinline__ bool couple_goes_on(Ctx* ctx, int max_groups) {
+  const int gdone = ++ctx->cs.groups;
+  return ctx->cs.cont && !ctx->cs.done && !ctx->wait_error && !ctx->nonfinite && gdone < max_groups;
+}
+__global__ void k_couple_continue(Ctx* ctx, cudaGraphConditionalHandle handle, int max_groups) {
+  cudaGraphSetConditional(handle, couple_goes_on(ctx, max_groups) ? 1u : 0u);
 }
 // the group's loop goes on while any member's does (done members' blocks
 // return at once in every group launch)
 template <typename T>
-__global__ void k_group_continue(const __grid_constant__ GroupPtrs<T> ga, int m, cudaGraphConditionalHandle handle) {
+__global__ void k_group_continue(const __grid_constant__ GroupPtrs<T> ga, int m, cudaGraphConditionalHandle handle,
+                                 int max_groups) {
   unsigned int c = 0;
-  for (int q = 0; q < m; q++) c |= ga.ctx[q]->cs.cont ? 1u : 0u;
+  for (int q = 0; q < m; q++) c |= couple_goes_on(ga.ctx[q], max_groups) ? 1u : 0u;
   cudaGraphSetConditional(handle, c);
 }
 

@@ -134,7 +134,9 @@ int autotune(lcs_batch* b) {
     best.share = share;
     best.probe_ms = 1e300;
     const int nz = ci.dims[2];
-    const int32_t rows_c[] = {13, 8, 5};
+    // tile rows: FP32 also has 29-row tiles (two rows a warp)
+    std::vector<int32_t> rows_c = {13, 8, 5};
+    if (ci.precision == LCS_PRECISION_FP32_MIXED) rows_c.insert(rows_c.begin(), 29);
     std::vector<int32_t> zc_c = {0};
     for (int d : {1, 2, 4})
       if (nz / d >= 8) zc_c.push_back((nz + 2) / d + 2);

@@ -52,9 +52,10 @@ from lcs_b200.workloads import WORKLOADS, host_inputs, load_engine, make_run_con
 OTHER_WORKLOADS = ("batch64", "serve", "makeindex", "couple256")
 
 # DRAM bytes (read + write) per interior cell of one launch of the sweep
-# kernel, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
-# of two sweep launches at 256^3: not measured in the run that reports them.
-SWEEP_DRAM_BYTES_PER_CELL = {"fp64": 69.6, "fp32-mixed": 36.3}
+# kernel, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum) of
+# a D2 sweep (box 0:n+2) at 256^3, one per precision: not measured in the run
+# that reports them.
+SWEEP_DRAM_BYTES_PER_CELL = {"fp64": 67.8, "fp32-mixed": 35.0}
 SWEEP_KERNELS = ("hsmac_rw", "hsmac_tma", "hsmac_fused")
 # FP64 operations per interior cell of one rhs!+update! launch (k_rhs, both
 # stages alike): smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on
@@ -189,8 +190,8 @@ def sweep_roofline(tot, n3, precision, peak, peak_kind):
     return {"kernel": k, "bound": "hbm", "achieved": ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": (ach / peak) if ach else None, "traffic": SWEEP_DRAM_BYTES_PER_CELL[precision] * n3,
             "traffic_source": "not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum per "
-                              f"interior cell of a 256^3 capture of the same kernel "
-                              f"({SWEEP_DRAM_BYTES_PER_CELL[precision]} B), times n^3",
+                              f"interior cell of a 256^3 capture of the same kernel (a D2 sweep, "
+                              f"{SWEEP_DRAM_BYTES_PER_CELL[precision]} B), times n^3",
             "alg_bytes_per_launch": alg, "avg_launch_ms": avg, "launches_profiled": cnt}
 
 

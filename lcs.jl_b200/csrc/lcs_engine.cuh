@@ -1276,8 +1276,10 @@ class Engine : public EngineBase {
     for (int s = 0; s < cfg.n_species; s++) {
       double dmax = 0.0;
       if (sp[s].n > 0) {
-        LCS_TRY(launch("max_diam", k_max_reduce, dim3(1), dim3(256), 0, (const double*)sp[s].p[LCS_PROP_DIAM], sp[s].n,
-                       stage));
+        const unsigned int nb = blocks_for(sp[s].n, 256, 148 * 4);
+        LCS_TRY(launch("max_diam", k_max_partial, dim3(nb), dim3(256), 0, (const double*)sp[s].p[LCS_PROP_DIAM], sp[s].n,
+                       partials));
+        LCS_TRY(launch("max_diam", k_max_reduce, dim3(1), dim3(256), 0, (const double*)partials, (int64_t)nb, stage));
         LCS_TRY(copy(&hctx->scal[7], stage, sizeof(double), cudaMemcpyDeviceToHost));
         LCS_CUDA(cudaStreamSynchronize(stream));
         dmax = hctx->scal[7];

@@ -1499,6 +1499,16 @@ __global__ void k_particles_init_velocity(const Ctx* __restrict__ ctx, Grid g, i
   sp.p[8][p] = interp<T>((const T*)ctx->vel[kSetUs][2], g, zmapping(x, y, z, pc.dx, pc.dy, pc.dz));
 }
 
+// max(0, a[0..n)) (maximum(diams) of particles/timestep.jl) in two passes:
+// block maxima over a grid-stride range, then the maximum of the blocks'.
+__global__ void __launch_bounds__(256) k_max_partial(const double* __restrict__ a, int64_t n,
+                                                      double* __restrict__ partials) {
+  __shared__ double sh[8];
+  double v = 0.0;
+  for (int64_t q = (int64_t)blockIdx.x * 256 + threadIdx.x; q < n; q += (int64_t)gridDim.x * 256) v = jl_max(v, a[q]);
+  const double m = block_max<256>(v, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = m;
+}
 __global__ void __launch_bounds__(256) k_max_reduce(const double* __restrict__ a, int64_t n, double* __restrict__ out) {
   __shared__ double sh[8];
   double v = 0.0;

@@ -526,15 +526,20 @@ def run_batch(args):
     b.step(max(1, args.warmup))
     import ctypes as C
 
+    def launch_total():
+        tot = 0
+        for e in b.members:
+            n = C.c_int64()
+            e._check(e.lib.lcs_launch_count(e.handle, C.byref(n)))
+            tot += n.value
+        return tot
+
+    l0 = launch_total()
     t0 = time.perf_counter()
     logs = b.step(args.steps)
     batch_s = time.perf_counter() - t0
+    launches = launch_total() - l0
     sweeps = float(np.mean([lg["couple1"]["sweeps"] + lg["couple2"]["sweeps"] for ml in logs for lg in ml]))
-    launches = 0
-    for e in b.members:
-        n = C.c_int64()
-        e._check(e.lib.lcs_launch_count(e.handle, C.byref(n)))
-        launches += n.value
     b.close()
     # the same members one at a time (each on its own handle)
     seq_steps = max(1, min(args.steps, 3))
@@ -558,6 +563,10 @@ def run_batch(args):
                    "cells": int(cells), "particles": int(parts_total), "precision": "fp32-mixed"},
         "particle_steps_per_s": parts_total * args.steps / batch_s,
         "hsmac_sweeps_per_member_step": sweeps,
+        "graph_kernel_nodes_per_step": launches / args.steps,
+        "graph_kernel_nodes_note": "kernel launches captured in the step graphs of all members and groups, the "
+                                   "body of each HSMAC WHILE loop counted once",
+        "groups": len(shapes),
         "sequential": {"value": seq_value, "steps": seq_steps, "note": "the members one after another, each alone"},
         "batch_vs_sequential": value / seq_value,
         "autotune": {"create_s": create_s, "chosen": shapes},

@@ -626,13 +626,12 @@ class Engine : public EngineBase {
 
   // ------------------------------------------------------------ primitives
   int fill(int set, bool withP, int r, int full) {
-    if (grp && withP) return fail(LCS_EINVAL, "group fills carry no P");
     FillArgs fa;
     memset(&fa, 0, sizeof fa);
     fa.nf = 0;
     if (set >= 0)
       for (int q = 0; q < 3; q++) { fa.set[fa.nf] = set; fa.comp[fa.nf] = q; fa.ptr[fa.nf] = nullptr; fa.nf++; }
-    if (withP) { fa.set[fa.nf] = -1; fa.comp[fa.nf] = 0; fa.ptr[fa.nf] = P; fa.nf++; }
+    if (withP) { fa.set[fa.nf] = -1; fa.comp[fa.nf] = 0; fa.ptr[fa.nf] = P; fa.nf++; }  // a group fill: each member's P
     const int64_t total = fill_count(g, r, full);
     if (total >= INT32_MAX) return fail(LCS_EINVAL, "halo too large for 32-bit fill indices");
     if (grp)
@@ -2089,10 +2088,45 @@ struct EngineGroup : GroupBase {
   std::vector<int64_t> per_step;
   std::vector<int> gens;
   cudaEvent_t ready = nullptr;
+  GroupMember<T>* gm = nullptr;  // the members' arguments of the group-wide launches (device)
   ~EngineGroup() override {
     if (mem.size()) cudaStreamSynchronize(mem[0]->stream);
     drop();
     if (ready) cudaEventDestroy(ready);
+    if (gm) cudaFree(gm);
+  }
+  // The members' arguments for the group-wide launches, uploaded once.
+  int member_args() {
+    const int M = (int)mem.size();
+    if (!gm) LCS_CUDA(cudaMalloc(&gm, (size_t)M * sizeof(GroupMember<T>)));
+    std::vector<GroupMember<T>> h(M);
+    memset(h.data(), 0, h.size() * sizeof(GroupMember<T>));
+    for (int q = 0; q < M; q++) {
+      Engine<T>* m = mem[q];
+      GroupMember<T>& a = h[q];
+      a.ctx = m->dctx;
+      a.P = m->P;
+      a.partials = m->partials;
+      for (int c = 0; c < 3; c++) a.dU[c] = m->dU[c];
+      a.logs = m->dlogs;
+      a.logs_cap = (int)m->plan.logs_cap;
+      a.itrmax = m->cfg.itrmax;
+      a.nspecies = m->cfg.mode == LCS_MODE_FLOW_PARTICLE ? m->cfg.n_species : 0;
+      a.rc = m->rc;
+      a.dc = m->dc;
+      a.pc = m->pc;
+      a.power = m->cfg.power;
+      for (int sp = 0; sp < a.nspecies; sp++) a.sp[sp] = m->sp[sp];
+    }
+    LCS_CUDA(cudaMemcpy(gm, h.data(), h.size() * sizeof(GroupMember<T>), cudaMemcpyHostToDevice));
+    return LCS_OK;
+  }
+  // one-thread work of every member (k_member_op_group: 0 step_begin,
+  // 1 set_stage_dt, 2 couple_reset, 3 couple_log, 4 step_end)
+  int member_op(int what, int stage, const char* label) {
+    const int M = (int)mem.size();
+    return mem[0]->launch(label, k_member_op_group<T>, dim3((M + 63) / 64), dim3(64), 0, (const GroupMember<T>*)gm, M,
+                          what, stage);
   }
   void drop() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -2110,8 +2144,7 @@ struct EngineGroup : GroupBase {
   int couple_nodes(int stage) {
     Engine<T>* L = mem[0];
     const int set = stage == 1 ? kSetUs2 : kSetUs;
-    for (auto* m : mem)
-      LCS_GTRY(m, m->launch("couple_reset", k_couple_reset, dim3(1), dim3(1), 0, m->dctx, m->cfg.itrmax));
+    LCS_GTRY(L, member_op(2, stage, "couple_reset"));
     cudaStream_t s = L->stream;
     cudaStreamCaptureStatus st;
     cudaGraph_t gr;
@@ -2149,31 +2182,78 @@ struct EngineGroup : GroupBase {
     cudaStreamDestroy(side);
     if (rc2 != LCS_OK) return rc2;
     LCS_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
-    for (auto* m : mem) LCS_GTRY(m, m->launch("couple_log", k_couple_log, dim3(1), dim3(1), 0, m->dctx, stage));
+    LCS_GTRY(L, member_op(3, stage, "couple_log"));
     return LCS_OK;
   }
+  // One step of every member: each per-member kernel of Engine::timestep_kernels
+  // and evolve_kernels as one group-wide launch (members' blocks side by side),
+  // the couples as the group's WHILE loops.  The rc-energy forcing keeps one
+  // launch sequence per member.
   int capture_step() {
-    for (auto* m : mem) LCS_GTRY(m, m->timestep_kernels(0, nullptr));
-    for (auto* m : mem) LCS_GTRY(m, m->launch("step_begin", k_step_begin, dim3(1), dim3(1), 0, m->dctx));
+    Engine<T>* L = mem[0];
+    const int M = (int)mem.size();
+    const Grid& g = L->g;
+    const int64_t ni = (int64_t)g.n[0] * g.n[1] * g.n[2];
+    const unsigned int nb = Engine<T>::blocks_for(ni, 256, 148 * 8);
+    L->grp = &mem;
+    // timestep!: FaceHalo fill, the CFL maxima and dt (flows/timestep.jl, timestep.jl)
+    int rc2 = L->fill(kSetUs, false, g.h, 0);
+    if (rc2 == LCS_OK)
+      rc2 = L->launch("cfl_max", k_cfl_max_group<T>, dim3(nb, M), dim3(256), 0, (const GroupMember<T>*)gm, g);
+    if (rc2 == LCS_OK)
+      rc2 = L->launch("cfl_finalize", k_cfl_finalize_group<T>, dim3(M), dim3(256), 0, (const GroupMember<T>*)gm, (int)nb);
+    L->grp = nullptr;
+    LCS_GTRY(L, rc2);
+    LCS_GTRY(L, member_op(0, 0, "step_begin"));
+    bool lf = true, any_forcing = false;
+    int nspec = 0;
+    int64_t np_max = 0;
+    for (auto* m : mem) {
+      lf = lf && m->cfg.forcing == LCS_FORCING_LINEAR_POWER;
+      any_forcing = any_forcing || m->cfg.forcing != LCS_FORCING_NO;
+      if (m->cfg.mode == LCS_MODE_FLOW_PARTICLE) {
+        nspec = std::max(nspec, (int)m->cfg.n_species);
+        for (int q = 0; q < m->cfg.n_species; q++) np_max = std::max<int64_t>(np_max, m->sp[q].n);
+      }
+    }
     for (int stage = 1; stage <= 2; stage++) {
       const int set = stage == 1 ? kSetUs : kSetUs2;
-      for (auto* m : mem) {
-        LCS_GTRY(m, m->set_stage_dt(stage));
-        LCS_GTRY(m, m->fill(set, true, m->g.h, 1));
-        LCS_GTRY(m, m->particles_stage(stage, 7, 1, 0.0));
-        LCS_GTRY(m, m->rhs_kernel(set, stage == 1 ? kSetUs2 : kSetUs, 1, 1, 0.0));
-        if (stage == 2) LCS_GTRY(m, m->forcing_stage());
+      LCS_GTRY(L, member_op(1, stage, "stage_dt"));
+      L->grp = &mem;
+      rc2 = L->fill(set, true, g.h, 1);  // synchalo!(FullHalo(grid), (Us.., P))
+      L->grp = nullptr;
+      LCS_GTRY(L, rc2);
+      for (int q = 0; q < nspec && np_max > 0; q++)  // boundary!, motion!, update! of species q of every member
+        LCS_GTRY(L, L->launch("particles", k_particles_group<T>, dim3((unsigned)((np_max + 255) / 256), M), dim3(256), 0,
+                              (const GroupMember<T>*)gm, g, q, stage, 7));
+      LCS_GTRY(L, L->launch("rhs_update", k_rhs_group<T>, dim3((g.n[0] + 127) / 128, g.n[1], g.n[2] * M), dim3(128), 0,
+                            (const GroupMember<T>*)gm, g, set, stage == 1 ? kSetUs2 : kSetUs, (int)kSetUs, 1, 1));
+      if (stage == 2 && any_forcing) {
+        if (lf) {  // forcing!(::ConstantPowerLF) of every member (lf.jl:27-106)
+          L->grp = &mem;
+          rc2 = L->fill(kSetUs, false, g.h, 1);
+          L->grp = nullptr;
+          LCS_GTRY(L, rc2);
+          LCS_GTRY(L, L->launch("lf_sums", k_lf_sums_group<T>, dim3(nb, M), dim3(256), 0, (const GroupMember<T>*)gm, g));
+          LCS_GTRY(L, L->launch("lf_coef", k_lf_coef_group<T>, dim3(M), dim3(256), 0, (const GroupMember<T>*)gm, (int)nb,
+                                (double)ni));
+          LCS_GTRY(L, L->launch("lf_apply", k_lf_apply_group<T>, dim3(nb, M), dim3(256), 0, (const GroupMember<T>*)gm, g));
+          LCS_GTRY(L, L->launch("power_mean", k_power_finalize_group<T>, dim3(M), dim3(256), 0, (const GroupMember<T>*)gm,
+                                (int)nb, (double)ni));
+        } else {
+          for (auto* m : mem) LCS_GTRY(m, m->forcing_stage());
+        }
       }
       LCS_TRY(couple_nodes(stage));
     }
-    for (auto* m : mem)
-      LCS_GTRY(m, m->launch("step_end", k_step_end, dim3(1), dim3(1), 0, m->dctx, m->dlogs, (int)m->plan.logs_cap));
+    LCS_GTRY(L, member_op(4, 0, "step_end"));
     return LCS_OK;
   }
 #undef LCS_GTRY
   int build() {
     Engine<T>* L = mem[0];
     cudaStream_t s = L->stream;
+    LCS_TRY(member_args());
     std::vector<cudaStream_t> saved(mem.size());
     LCS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
     for (size_t q = 0; q < mem.size(); q++) {

@@ -84,7 +84,7 @@ struct FillArgs {
 
 template <typename T>
 __device__ __forceinline__ void fill_halo_body(const Ctx* __restrict__ ctx, const Grid& g, const FillArgs& fa, int r,
-                                               int full, int64_t total) {
+                                               int full, int64_t total, T* Pm = nullptr) {
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
   const int wx = full ? nx + 2 * r : nx, wy = full ? ny + 2 * r : ny;
   const int bx = full ? 1 - r : 1, by = full ? 1 - r : 1;
@@ -94,7 +94,7 @@ __device__ __forceinline__ void fill_halo_body(const Ctx* __restrict__ ctx, cons
   T* f[4];
 #pragma unroll
   for (int q = 0; q < 4; q++)
-    f[q] = q < fa.nf ? (T*)(fa.set[q] >= 0 ? ctx->vel[fa.set[q]][fa.comp[q]] : fa.ptr[q]) : nullptr;
+    f[q] = q < fa.nf ? (T*)(fa.set[q] >= 0 ? ctx->vel[fa.set[q]][fa.comp[q]] : (Pm ? Pm : (T*)fa.ptr[q])) : nullptr;
   // total < 2^31 (checked on the host): 32-bit index arithmetic
   const int tot = (int)total;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
@@ -186,14 +186,14 @@ __device__ __forceinline__ T rhs_component(const T* __restrict__ U, const T* __r
 
 // in_set: velocity set read by rhs; out_set: set written (mode 1); u0_set: U0
 template <typename T>
-__global__ void __launch_bounds__(256) k_rhs(const Ctx* __restrict__ ctx, Grid g, const T* __restrict__ P, int in_set,
-                                             int out_set, int u0_set, int mode, T* __restrict__ dU,
-                                             T* __restrict__ dV, T* __restrict__ dW, RhsCoef cf, int use_stage_dt,
-                                             double dt_arg) {
+__device__ __forceinline__ void rhs_body(const Ctx* __restrict__ ctx, const Grid& g, const T* __restrict__ P,
+                                         int in_set, int out_set, int u0_set, int mode, T* __restrict__ dU,
+                                         T* __restrict__ dV, T* __restrict__ dW, const RhsCoef& cf, int use_stage_dt,
+                                         double dt_arg, int kz) {
   const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y;
-  const int k = 1 + blockIdx.z;
+  const int k = 1 + kz;
   if (i > nx || j > ny || k > nz) return;
   const T* U = (const T*)ctx->vel[in_set][0];
   const T* V = (const T*)ctx->vel[in_set][1];
@@ -222,6 +222,13 @@ __global__ void __launch_bounds__(256) k_rhs(const Ctx* __restrict__ ctx, Grid g
     Vo[c] = v + dv;
     Wo[c] = w + dw;
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_rhs(const Ctx* __restrict__ ctx, Grid g, const T* __restrict__ P, int in_set,
+                                             int out_set, int u0_set, int mode, T* __restrict__ dU,
+                                             T* __restrict__ dV, T* __restrict__ dW, RhsCoef cf, int use_stage_dt,
+                                             double dt_arg) {
+  rhs_body<T>(ctx, g, P, in_set, out_set, u0_set, mode, dU, dV, dW, cf, use_stage_dt, dt_arg, (int)blockIdx.z);
 }
 
 // update! alone (the reference's separate kernel), reading dUdts.
@@ -577,7 +584,7 @@ __global__ void __launch_bounds__(256) k_hsmac_faces_group(const __grid_constant
 template <typename T>
 __global__ void __launch_bounds__(256) k_fill_halo_group(const __grid_constant__ GroupPtrs<T> ga, Grid g, FillArgs fa,
                                                          int r, int full, int64_t total) {
-  fill_halo_body<T>(ga.ctx[blockIdx.y], g, fa, r, full, total);
+  fill_halo_body<T>(ga.ctx[blockIdx.y], g, fa, r, full, total, ga.P[blockIdx.y]);  // P: the member's own
 }
 
 // Fused red-black sweep over the box D with the velocities ping-ponged:
@@ -795,7 +802,7 @@ __global__ void __launch_bounds__(TX * TY) k_hsmac_fused(Ctx* __restrict__ ctx, 
 }
 
 // Reset the couple state before a couple! call.
-__global__ void k_couple_reset(Ctx* ctx, int itrmax) {
+__device__ __forceinline__ void couple_reset_body(Ctx* ctx, int itrmax) {
   ctx->cs.itr = 0;
   ctx->cs.sweeps = 0;
   ctx->cs.done = 0;
@@ -805,9 +812,10 @@ __global__ void k_couple_reset(Ctx* ctx, int itrmax) {
   ctx->cs.groups = 0;
   ctx->ticket = 0;
 }
+__global__ void k_couple_reset(Ctx* ctx, int itrmax) { couple_reset_body(ctx, itrmax); }
 
 // Record the couple result into the step log (stage 1 or 2).
-__global__ void k_couple_log(Ctx* ctx, int stage) {
+__device__ __forceinline__ void couple_log_body(Ctx* ctx, int stage) {
   if (stage == 1) {
     ctx->cur.itr1 = ctx->cs.itr;
     ctx->cur.sweeps1 = ctx->cs.sweeps;
@@ -818,6 +826,7 @@ __global__ void k_couple_log(Ctx* ctx, int stage) {
     ctx->cur.div2 = ctx->cs.div;
   }
 }
+__global__ void k_couple_log(Ctx* ctx, int stage) { couple_log_body(ctx, stage); }
 
 // WHILE-node condition of the device-resident couple loop.
 // The loop goes on while the exit test says so, no sweep has stopped the
@@ -846,7 +855,7 @@ __global__ void k_group_continue(const __grid_constant__ GroupPtrs<T> ga, int m,
 // time step (src/flows/timestep.jl:18-65; src/timestep.jl:14-27)
 // --------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_cfl_max(const Ctx* __restrict__ ctx, Grid g, double* __restrict__ partials) {
+__device__ __forceinline__ void cfl_max_body(const Ctx* __restrict__ ctx, const Grid& g, double* __restrict__ partials) {
   __shared__ double sh[8];
   const T* U = (const T*)ctx->vel[kSetUs][0];
   const T* V = (const T*)ctx->vel[kSetUs][1];
@@ -874,6 +883,10 @@ __global__ void __launch_bounds__(256) k_cfl_max(const Ctx* __restrict__ ctx, Gr
     partials[3 * blockIdx.x + 1] = b;
     partials[3 * blockIdx.x + 2] = c;
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_cfl_max(const Ctx* __restrict__ ctx, Grid g, double* __restrict__ partials) {
+  cfl_max_body<T>(ctx, g, partials);
 }
 
 // --------------------------------------------------------------------------
@@ -1022,8 +1035,8 @@ struct DtCoef {
 
 // dt = min(dtmax, cfl dx/umax, cfl dy/vmax, cfl dz/wmax, 0.5 (dx/2)^2 / (1/Re))
 // [, particle dt]; writes ctx->dt (and *out).
-__global__ void __launch_bounds__(256) k_cfl_finalize(Ctx* ctx, const double* __restrict__ partials, int nb, DtCoef c,
-                                                      int flow_only, double* out) {
+__device__ __forceinline__ void cfl_finalize_body(Ctx* ctx, const double* __restrict__ partials, int nb,
+                                                  const DtCoef& c, int flow_only, double* out) {
   __shared__ double sh[8];
   double m[3];
   for (int a = 0; a < 3; a++) {
@@ -1047,13 +1060,17 @@ __global__ void __launch_bounds__(256) k_cfl_finalize(Ctx* ctx, const double* __
     if (out) *out = d;
   }
 }
+__global__ void __launch_bounds__(256) k_cfl_finalize(Ctx* ctx, const double* __restrict__ partials, int nb, DtCoef c,
+                                                      int flow_only, double* out) {
+  cfl_finalize_body(ctx, partials, nb, c, flow_only, out);
+}
 
 // --------------------------------------------------------------------------
 // forcing: linear-power (src/flows/forcings/lf.jl:27-106)
 // pass 1: sums of |u_cc|^2, U, V, W over the interior; pass 2: apply.
 // --------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_lf_sums(const Ctx* __restrict__ ctx, Grid g, double* __restrict__ partials) {
+__device__ __forceinline__ void lf_sums_body(const Ctx* __restrict__ ctx, const Grid& g, double* __restrict__ partials) {
   __shared__ double sh[8];
   const T* U = (const T*)ctx->vel[kSetUs][0];
   const T* V = (const T*)ctx->vel[kSetUs][1];
@@ -1084,10 +1101,14 @@ __global__ void __launch_bounds__(256) k_lf_sums(const Ctx* __restrict__ ctx, Gr
     partials[4 * blockIdx.x + 3] = d;
   }
 }
+template <typename T>
+__global__ void __launch_bounds__(256) k_lf_sums(const Ctx* __restrict__ ctx, Grid g, double* __restrict__ partials) {
+  lf_sums_body<T>(ctx, g, partials);
+}
 
 // scal[1..4] = means (u2, u, v, w); scal[5] = A = p0 / (2e)
-__global__ void __launch_bounds__(256) k_lf_coef(Ctx* ctx, const double* __restrict__ partials, int nb, double count,
-                                                 double p0) {
+__device__ __forceinline__ void lf_coef_body(Ctx* ctx, const double* __restrict__ partials, int nb, double count,
+                                             double p0) {
   __shared__ double sh[8];
   double m[4];
   for (int a = 0; a < 4; a++) {
@@ -1105,9 +1126,13 @@ __global__ void __launch_bounds__(256) k_lf_coef(Ctx* ctx, const double* __restr
     ctx->scal[5] = p0 / (2.0 * e);
   }
 }
+__global__ void __launch_bounds__(256) k_lf_coef(Ctx* ctx, const double* __restrict__ partials, int nb, double count,
+                                                 double p0) {
+  lf_coef_body(ctx, partials, nb, count, p0);
+}
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_lf_apply(Ctx* __restrict__ ctx, Grid g, double* __restrict__ partials) {
+__device__ __forceinline__ void lf_apply_body(Ctx* __restrict__ ctx, const Grid& g, double* __restrict__ partials) {
   __shared__ double sh[8];
   T* U = (T*)ctx->vel[kSetUs][0];
   T* V = (T*)ctx->vel[kSetUs][1];
@@ -1133,10 +1158,14 @@ __global__ void __launch_bounds__(256) k_lf_apply(Ctx* __restrict__ ctx, Grid g,
   const double s = block_sum<256>(sp, sh);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
+template <typename T>
+__global__ void __launch_bounds__(256) k_lf_apply(Ctx* __restrict__ ctx, Grid g, double* __restrict__ partials) {
+  lf_apply_body<T>(ctx, g, partials);
+}
 
 // mean of the per-cell power -> ctx->scal[6], and the step log
-__global__ void __launch_bounds__(256) k_power_finalize(Ctx* ctx, const double* __restrict__ partials, int nb,
-                                                        double count, double e10) {
+__device__ __forceinline__ void power_finalize_body(Ctx* ctx, const double* __restrict__ partials, int nb,
+                                                    double count, double e10) {
   __shared__ double sh[8];
   const double s = sum_partials<256>(partials, nb, sh);
   if (threadIdx.x == 0) {
@@ -1144,6 +1173,10 @@ __global__ void __launch_bounds__(256) k_power_finalize(Ctx* ctx, const double* 
     ctx->cur.p = s / count;
     ctx->cur.e10 = e10;
   }
+}
+__global__ void __launch_bounds__(256) k_power_finalize(Ctx* ctx, const double* __restrict__ partials, int nb,
+                                                        double count, double e10) {
+  power_finalize_body(ctx, partials, nb, count, e10);
 }
 
 // --------------------------------------------------------------------------
@@ -1411,8 +1444,9 @@ __device__ __forceinline__ void species_arrays(const Ctx* __restrict__ ctx, int 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_particles(const Ctx* __restrict__ ctx, Grid g, int s, SpeciesDev sp,
-                                                   PartCoef pc, int stage, int modes, int use_stage_dt, double dt_arg) {
+__device__ __forceinline__ void particles_body(const Ctx* __restrict__ ctx, const Grid& g, int s, SpeciesDev sp,
+                                               const PartCoef& pc, int stage, int modes, int use_stage_dt,
+                                               double dt_arg) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= sp.n) return;
   species_arrays(ctx, s, sp);
@@ -1485,6 +1519,11 @@ __global__ void __launch_bounds__(256) k_particles(const Ctx* __restrict__ ctx, 
       sp.p[(stage == 1 ? 9 : 6) + a][p] = u0 + dt * dudt[a];
     }
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_particles(const Ctx* __restrict__ ctx, Grid g, int s, SpeciesDev sp,
+                                                   PartCoef pc, int stage, int modes, int use_stage_dt, double dt_arg) {
+  particles_body<T>(ctx, g, s, sp, pc, stage, modes, use_stage_dt, dt_arg);
 }
 
 // New init kind: particle velocity = trilinear interpolation of Us.
@@ -1592,21 +1631,116 @@ __global__ void k_convert_out(double* __restrict__ dst, const T* __restrict__ sr
 // --------------------------------------------------------------------------
 // step bookkeeping (src/evolve.jl:10-13, src/state.jl:37-38)
 // --------------------------------------------------------------------------
-__global__ void k_set_stage_dt(Ctx* ctx, int stage) { ctx->scal[0] = stage == 1 ? 0.5 * ctx->dt : ctx->dt; }
+__device__ __forceinline__ void stage_dt_body(Ctx* ctx, int stage) {
+  ctx->scal[0] = stage == 1 ? 0.5 * ctx->dt : ctx->dt;  // dtrk (src/state.jl:37-38)
+}
+__global__ void k_set_stage_dt(Ctx* ctx, int stage) { stage_dt_body(ctx, stage); }
 __global__ void k_set_scalar(double* dst, double v) { *dst = v; }
 __global__ void k_set_debug_wait(Ctx* ctx, int kind) { ctx->debug_wait = kind; }
 __global__ void k_set_species_base(Ctx* ctx, int s, double* base) { ctx->sp_base[s] = base; }
-__global__ void k_step_begin(Ctx* ctx) {
+__device__ __forceinline__ void step_begin_body(Ctx* ctx) {
   ctx->cur.p = __longlong_as_double(0x7ff8000000000000LL);
   ctx->cur.e10 = __longlong_as_double(0x7ff8000000000000LL);
 }
-__global__ void k_step_end(Ctx* ctx, StepLog* logs, int cap) {
+__global__ void k_step_begin(Ctx* ctx) { step_begin_body(ctx); }
+__device__ __forceinline__ void step_end_body(Ctx* ctx, StepLog* logs, int cap) {
   ctx->step += 1;
   ctx->t += ctx->dt;
   ctx->cur.t = ctx->t;
   ctx->cur.step = ctx->step;
   ctx->cur.dt = ctx->dt;
   if (logs) logs[(ctx->step - 1) % cap] = ctx->cur;
+}
+__global__ void k_step_end(Ctx* ctx, StepLog* logs, int cap) { step_end_body(ctx, logs, cap); }
+
+// --------------------------------------------------------------------------
+// Batch groups: the per-member kernels of a step as group-wide launches, one
+// launch for all members.  Members share dims and halo; each member's own
+// arguments (context, P, partials, coefficients, particle arrays) come from a
+// device array indexed by blockIdx.y (blockIdx.z / nz for the rhs, blockIdx.x
+// for the one-block kernels), and blockIdx.x and gridDim.x keep the meaning
+// they have in the member's own launch.  So each member computes exactly what
+// its own kernels compute, and its reductions group their partial sums in the
+// same order.
+// --------------------------------------------------------------------------
+template <typename T>
+struct GroupMember {
+  Ctx* ctx;
+  T* P;
+  double* partials;
+  T* dU[3];
+  StepLog* logs;
+  int logs_cap;
+  int itrmax;
+  int nspecies;  // 0 in FlowMode
+  int pad_;
+  RhsCoef rc;
+  DtCoef dc;
+  PartCoef pc;
+  double power;  // linear-power P0
+  SpeciesDev sp[LCS_MAX_SPECIES];
+};
+template <typename T>
+__global__ void __launch_bounds__(256) k_cfl_max_group(const GroupMember<T>* __restrict__ gm, Grid g) {
+  const GroupMember<T>& m = gm[blockIdx.y];
+  cfl_max_body<T>(m.ctx, g, m.partials);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_cfl_finalize_group(const GroupMember<T>* __restrict__ gm, int nb) {
+  const GroupMember<T>& m = gm[blockIdx.x];
+  cfl_finalize_body(m.ctx, m.partials, nb, m.dc, 0, nullptr);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_rhs_group(const GroupMember<T>* __restrict__ gm, Grid g, int in_set,
+                                                   int out_set, int u0_set, int mode, int use_stage_dt) {
+  const int nz = g.n[2];
+  const GroupMember<T>& m = gm[blockIdx.z / nz];
+  rhs_body<T>(m.ctx, g, m.P, in_set, out_set, u0_set, mode, m.dU[0], m.dU[1], m.dU[2], m.rc, use_stage_dt, 0.0,
+              (int)(blockIdx.z % nz));
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_particles_group(const GroupMember<T>* __restrict__ gm, Grid g, int s,
+                                                         int stage, int modes) {
+  const GroupMember<T>& m = gm[blockIdx.y];
+  if (s >= m.nspecies) return;
+  particles_body<T>(m.ctx, g, s, m.sp[s], m.pc, stage, modes, 1, 0.0);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_lf_sums_group(const GroupMember<T>* __restrict__ gm, Grid g) {
+  const GroupMember<T>& m = gm[blockIdx.y];
+  lf_sums_body<T>(m.ctx, g, m.partials);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_lf_coef_group(const GroupMember<T>* __restrict__ gm, int nb, double count) {
+  const GroupMember<T>& m = gm[blockIdx.x];
+  lf_coef_body(m.ctx, m.partials, nb, count, m.power);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_lf_apply_group(const GroupMember<T>* __restrict__ gm, Grid g) {
+  const GroupMember<T>& m = gm[blockIdx.y];
+  lf_apply_body<T>(m.ctx, g, m.partials);
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_power_finalize_group(const GroupMember<T>* __restrict__ gm, int nb,
+                                                              double count) {
+  const GroupMember<T>& m = gm[blockIdx.x];
+  power_finalize_body(m.ctx, m.partials, nb, count, (double)NAN);
+}
+// the one-thread kernels of a step, one thread per member: what 0 step_begin,
+// 1 set_stage_dt(stage), 2 couple_reset, 3 couple_log(stage), 4 step_end
+template <typename T>
+__global__ void k_member_op_group(const GroupMember<T>* __restrict__ gm, int M, int what, int stage) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= M) return;
+  const GroupMember<T>& m = gm[q];
+  Ctx* ctx = m.ctx;
+  switch (what) {
+    case 0: step_begin_body(ctx); break;
+    case 1: stage_dt_body(ctx, stage); break;
+    case 2: couple_reset_body(ctx, m.itrmax); break;
+    case 3: couple_log_body(ctx, stage); break;
+    default: step_end_body(ctx, m.logs, m.logs_cap);
+  }
 }
 
 }  // namespace

@@ -24,9 +24,8 @@
 
 #include "lcs_base.h"
 #include "lcs_kernels.cuh"
-#include "lcs_hsmac_tma.cuh"
+#include "lcs_tma.cuh"
 #include "lcs_hsmac_rw.cuh"
-#include "lcs_hsmac_rw4.cuh"
 #include "lcs_makeindex.cuh"
 #include "lcs_pstat.cuh"
 
@@ -302,88 +301,42 @@ class Engine : public EngineBase {
     dc.with_particles = c.mode == LCS_MODE_FLOW_PARTICLE && c.n_species > 0;
     pc.dx = dx; pc.dy = dy; pc.dz = dz; pc.Re = Re;
     if (c.forcing == LCS_FORCING_RC_ENERGY) LCS_TRY(init_rcf());
-    // the TMA-fed sweeps serve red-black-fast (the production colouring): the
-    // row-warp kernel by default; LCS_B200_FUSED_SWEEP=tma selects the
-    // thread-per-item TMA kernel (FP64 only), =plain the plain-load sweep
+    // the TMA-fed row-warp sweep serves red-black-fast (the production
+    // colouring); LCS_B200_FUSED_SWEEP=plain selects the plain-load sweep
     const char* sweep = std::getenv("LCS_B200_FUSED_SWEEP");
     const std::string sw = sweep ? std::string(sweep) : std::string("rw");
-    constexpr bool f64 = std::is_same<T, double>::value;
-    use_tma = c.coloring == LCS_COLORING_RED_BLACK_FAST && sw != "plain";
-    use_rw = use_tma && !(f64 && sw == "tma");
+    use_rw = c.coloring == LCS_COLORING_RED_BLACK_FAST && sw != "plain";
     // the row-warp sweep addresses a field with 32-bit offsets
     if (use_rw && (uint64_t)g.pz * (uint64_t)(g.n[2] + 2 * g.h) >= (1ull << 32))
       return fail(LCS_EINVAL, "a field of 2^32 or more elements");
-    if (use_tma) LCS_TRY(init_tma());
+    if (use_rw) LCS_TRY(init_tma());
     LCS_TRY(init_faces());
     LCS_CUDA(cudaStreamSynchronize(stream));
     return LCS_OK;
   }
 
   // ---------------------------------------------------------- tensor maps
-  static constexpr int TNS = 4;
-  bool use_tma = false;
-  TensorMaps tmaps;
-  // tile shape of the TMA sweep: 0 = 64x8, 1 = 32x16, 2 = 32x8, 3 = 64x16
-  // (LCS_B200_TILE=64x8|32x16|32x8|64x16); LCS_B200_ZCHUNK forces the z chunk
-  int tile_variant = 0, zchunk_force = 0, TTX = 64, TTY = 8, tma_threads = 384;
-  size_t tma_smem = 0;
-  const void* tma_fn = nullptr;
+  // LCS_B200_ZCHUNK forces the z chunk of the row-warp sweep
+  int zchunk_force = 0;
   int init_tma() {
-    if (const char* t = std::getenv("LCS_B200_TILE")) {
-      const std::string v(t);
-      tile_variant = v == "32x16" ? 1 : v == "32x8" ? 2 : v == "64x16" ? 3 : 0;
-    }
     if (const char* z = std::getenv("LCS_B200_ZCHUNK")) zchunk_force = std::atoi(z);
-    if (std::is_same<T, double>::value) switch (tile_variant) {
-      case 1: TTX = 32; TTY = 16; tma_smem = TmaLayout<32, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 16, TNS>;
-              tma_threads = TmaThreads<32, 16>::NT; break;
-      case 2: TTX = 32; TTY = 8; tma_smem = TmaLayout<32, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<32, 8, TNS>;
-              tma_threads = TmaThreads<32, 8>::NT; break;
-      case 3: TTX = 64; TTY = 16; tma_smem = TmaLayout<64, 16, TNS>::total; tma_fn = (const void*)k_hsmac_tma<64, 16, TNS>;
-              tma_threads = TmaThreads<64, 16>::NT; break;
-      default: TTX = 64; TTY = 8; tma_smem = TmaLayout<64, 8, TNS>::total; tma_fn = (const void*)k_hsmac_tma<64, 8, TNS>;
-               tma_threads = TmaThreads<64, 8>::NT; break;
-    }
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     LCS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
     if (!fn || q != cudaDriverEntryPointSuccess) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled is unavailable");
     auto encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    const CUtensorMapDataType dtype =
-        std::is_same<T, double>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)(g.n[1] + 2 * g.h), (cuuint64_t)(g.n[2] + 2 * g.h)};
-    const cuuint64_t strides[2] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.pz * sizeof(T)};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const cuuint32_t vbox[3] = {(cuuint32_t)TTX + 4, (cuuint32_t)TTY + 4, 1};
-    const cuuint32_t pbox[3] = {(cuuint32_t)TTX, (cuuint32_t)TTY, 1};
-    if (std::is_same<T, double>::value && !use_rw) {  // the thread-per-item kernel (FP64)
-      for (int b = 0; b < kVelMaps; b++) {
-        CUresult r = encode(&tmaps.vel[b], dtype, 3, vel0[b / 3][b % 3], dims, strides, vbox, estr,
-                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (velocity %d) failed: %d", b, (int)r);
-      }
-      CUresult r = encode(&tmaps.P, dtype, 3, (void*)P, dims, strides, pbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (P) failed: %d", (int)r);
-      LCS_CUDA(cudaFuncSetAttribute(tma_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem));
-      LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tma_ctas_per_sm, tma_fn, tma_threads, tma_smem));
-      if (tma_ctas_per_sm < 1) return fail(LCS_ECUDA, "the TMA sweep does not fit on an SM");
-    }
     LCS_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, cfg.device));
     encode_fn = encode;
     if (use_rw) {
-      // row-warp sweep tile rows: LCS_B200_RW=13 (default: one CTA of 16 warps
-      // per SM, a row per warp, fastest at 512^3 in both precisions) | 8 | 5 |
-      // 29 (FP32 only: 16 warps of two rows each, faster at 256^3)
-      rw_variant = 0;
+      // row-warp sweep tile rows: FP64 13 (one CTA of 16 warps per SM, a row
+      // per warp); FP32 29 (16 warps of two rows each: 1019-1034 against
+      // 1127-1136 us a sweep at 512^3, 177-184 against 201-207 at 256^3);
+      // LCS_B200_RW=13 | 8 | 5 | 29 (FP32 only) chooses another
+      rw_variant = std::is_same<T, float>::value ? 3 : 0;
       if (const char* v = std::getenv("LCS_B200_RW")) {
         const std::string t(v);
         rw_variant = t == "8" ? 1 : t == "5" ? 2 : (t == "29" && std::is_same<T, float>::value) ? 3 : 0;
       }
-      const char* q4 = std::getenv("LCS_B200_RW4");
-      use_rw4 = std::is_same<T, float>::value && q4 && std::string(q4) == "1";
       LCS_TRY(init_rw_maps());
     }
     return LCS_OK;
@@ -391,9 +344,6 @@ class Engine : public EngineBase {
   // The row-warp sweep of the current rw_variant: kernel, shared memory,
   // occupancy and its tensor maps (box 64 x rows+4 and 64 x rows).
   int init_rw_maps() {
-    if constexpr (std::is_same<T, float>::value) {
-      if (use_rw4) return init_rw4_maps();
-    }
     switch (rw_variant) {
       case 1: RTY = 8; rw_smem = RwLayout<T, 8, 3>::total; rw_fn = (const void*)k_hsmac_rw<T, 8, 3>;
               rw_threads = RwLayout<T, 8, 3>::NT; break;
@@ -439,51 +389,13 @@ class Engine : public EngineBase {
     if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the row-warp sweep does not fit on an SM");
     return LCS_OK;
   }
-  // the quad sweep's kernels and tensor maps (box 128 x rows+4 and 128 x rows)
-  int init_rw4_maps() {
-    const void* grp_fn = nullptr;
-    switch (rw_variant) {
-      case 1: RTY = 8; rw_smem = Rw4Layout<8, 3>::total; rw_fn = (const void*)k_hsmac_rw4<8, 3>;
-              grp_fn = (const void*)k_hsmac_rw4_group<8, 3>; rw_threads = Rw4Layout<8, 3>::NT; break;
-      case 2: RTY = 5; rw_smem = Rw4Layout<5, 3>::total; rw_fn = (const void*)k_hsmac_rw4<5, 3>;
-              grp_fn = (const void*)k_hsmac_rw4_group<5, 3>; rw_threads = Rw4Layout<5, 3>::NT; break;
-      default: RTY = 13; rw_smem = Rw4Layout<13, 3>::total; rw_fn = (const void*)k_hsmac_rw4<13, 3>;
-               grp_fn = (const void*)k_hsmac_rw4_group<13, 3>; rw_threads = Rw4Layout<13, 3>::NT; break;
-    }
-    const CUtensorMapDataType dtype = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)(g.n[1] + 2 * g.h), (cuuint64_t)(g.n[2] + 2 * g.h)};
-    const cuuint64_t strides[2] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.pz * sizeof(T)};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const cuuint32_t rbox[3] = {(cuuint32_t)RW4_W, (cuuint32_t)RTY + 4, 1};
-    for (int b = 0; b < kVelMaps; b++) {
-      CUresult rr = encode_fn(&tmaps_rw4.vel[b], dtype, 3, vel0[b / 3][b % 3], dims, strides, rbox, estr,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (rr != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (quad velocity %d) failed: %d", b, (int)rr);
-    }
-    const cuuint32_t rpbox[3] = {(cuuint32_t)RW4_W, (cuuint32_t)RTY, 1};
-    CUresult rp = encode_fn(&tmaps_rw4.P, dtype, 3, (void*)P, dims, strides, rpbox, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (rp != CUDA_SUCCESS) return fail(LCS_ECUDA, "cuTensorMapEncodeTiled (quad P) failed: %d", (int)rp);
-    LCS_CUDA(cudaFuncSetAttribute(rw_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
-    LCS_CUDA(cudaFuncSetAttribute(grp_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rw_smem));
-    LCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rw_ctas_per_sm, rw_fn, rw_threads, rw_smem));
-    if (rw_ctas_per_sm < 1) return fail(LCS_ECUDA, "the quad row-warp sweep does not fit on an SM");
-    return LCS_OK;
-  }
   PFN_cuTensorMapEncodeTiled_v12000 encode_fn = nullptr;
-  int num_sms = 148, tma_ctas_per_sm = 1;
+  int num_sms = 148;
   bool use_rw = false;
   TensorMaps tmaps_rw;
   int rw_variant = 0, RTY = 13, rw_threads = 512, rw_ctas_per_sm = 1;
   size_t rw_smem = 0;
   const void* rw_fn = nullptr;
-  // FP32: the quad row-warp sweep (four cells per lane, tiles 120 wide),
-  // chosen by LCS_B200_RW4=1; measured slower than the pair sweep at 256^3
-  // (226 vs 213 us per sweep), so the pair sweep is the default
-  bool use_rw4 = false;
-  TensorMaps tmaps_rw4;
 
   // blocks of the cooperative face-phase kernel (0: twelve in-place launches)
   int face_grid = 0;
@@ -675,7 +587,7 @@ class Engine : public EngineBase {
   }
   int fused(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks = nullptr) {
     if (grp && !use_rw) return fail(LCS_EINVAL, "group sweeps need the row-warp sweep");
-    if (use_tma) return fused_tma(set, D, out, fill_r, part, finalize, group_end, nblocks);
+    if (use_rw) return fused_rw(set, D, out, fill_r, part, finalize, group_end, nblocks);
     const FusedGeom f = fused_geom(out);
     const int64_t nb = (int64_t)f.gx * f.gy * f.gz;
     if (nb > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
@@ -692,30 +604,21 @@ class Engine : public EngineBase {
   // split their work to fill every SM.
   double sm_share = 1.0;
   int share_slots(int slots) const { return std::max(1, (int)std::lround(slots * sm_share)); }
-  int pick_zchunk(int nzc, int ncols, int slots) const {
-    slots = share_slots(slots);
-    int best_nc = 1;
-    double best = 1e300;
-    for (int nc = 1; nc <= std::min(nzc, 64); nc++) {
-      const int zc = (nzc + nc - 1) / nc;
-      const int nch = (nzc + zc - 1) / zc;
-      const int64_t items = (int64_t)ncols * nch;
-      const double waves = std::ceil((double)items / slots);
-      const double cost = waves * (zc + 4);
-      if (cost < best - 1e-9) { best = cost; best_nc = nc; }
-    }
-    return zchunk_force > 0 ? std::min(zchunk_force, nzc) : (nzc + best_nc - 1) / best_nc;
-  }
   // Schedule of a row-warp sweep: chunks of zc planes per tile column, chunk
   // major, in full waves of the resident CTAs; the chunks of a last, partial
   // wave are split into q sub-ranges so that it fills the GPU too.  zc
   // minimises the cost in plane-steps: full waves x (zc + 4 warm-up/drain
-  // planes) + the last wave's (sub-range + 4).
+  // planes) + the last wave's (sub-range + 4), with chunks of at most
+  // kMaxChunk planes: CTAs that stream whole columns at once move through z in
+  // step and read the same few planes together, which measured far slower
+  // (512^3 FP32, 29-row tiles: 1484 us a sweep with 514-plane chunks, 1019-1034
+  // with 48-96).
+  static constexpr int kMaxChunk = 96;
   RwSched rw_schedule(int ncols, int nzc, int slots) const {
     slots = share_slots(slots);
     RwSched best{ncols, nzc, ncols, 1, ncols};
     double best_cost = 1e300;
-    for (int nc = 1; nc <= std::min(nzc, 64); nc++) {
+    for (int nc = std::max(1, (nzc + kMaxChunk - 1) / kMaxChunk); nc <= std::max(std::min(nzc, 64), 1); nc++) {
       const int zc = zchunk_force > 0 ? std::min(zchunk_force, nzc) : (nzc + nc - 1) / nc;
       const int nch = (nzc + zc - 1) / zc;
       const int items = ncols * nch;
@@ -735,9 +638,6 @@ class Engine : public EngineBase {
   int fused_rw(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
     if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
     const Box gb = bbox(out, cube(g, 1, 0));
-    if constexpr (std::is_same<T, float>::value) {
-      if (use_rw4) return fused_rw4(set, D, out, gb, part, finalize, group_end, nblocks);
-    }
     // first tile column: the largest x0 <= gb.lo[0] with x0-2 on a 16-byte
     // boundary (x0 odd in FP64, x0 = 3 mod 4 in FP32); tiles step by RW_TX = 60
     const int am = 16 / (int)sizeof(T), ar = am - 1;
@@ -763,54 +663,6 @@ class Engine : public EngineBase {
                             out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
       default: return launch("hsmac_rw", k_hsmac_rw<T, 13, kRwRing<T>>, grid, block, rw_smem, dctx, g, set, tmaps_rw, P,
                              D, out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
-    }
-  }
-  // FP32 quad sweep: tiles of RW4_TX x RTY whose first column x0 = 1 mod 4
-  // (x0-4 on a 16-byte boundary)
-  int fused_rw4(int set, Box D, Box out, Box gb, double* part, int finalize, int group_end, int* nblocks) {
-    int xo = gb.lo[0];
-    while (((xo % 4) + 4) % 4 != 1) xo--;
-    const int gx = (gb.hi[0] - xo + 1 + RW4_TX - 1) / RW4_TX, gy = (gb.len(1) + RTY - 1) / RTY;
-    const int nzc = gb.len(2), ncols = gx * gy;
-    const RwSched sc = rw_schedule(ncols, nzc, num_sms * rw_ctas_per_sm);
-    if (sc.nitems > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
-    if (nblocks) *nblocks = sc.nitems;
-    if (grp) {
-      const int M = (int)grp->size();
-      for (int m0 = 0; m0 < M; m0 += kGroupMax) {
-        const int mc = std::min(kGroupMax, M - m0);
-        GroupRwArgs<float> ga;
-        memset(&ga, 0, sizeof ga);
-        for (int q = 0; q < mc; q++) {
-          Engine<T>* e = (*grp)[m0 + q];
-          ga.tm[q] = e->tmaps_rw4;
-          ga.ctx[q] = e->dctx;
-          ga.P[q] = (float*)e->P;
-          ga.partials[q] = e->partials;
-        }
-        const dim3 grid(sc.nitems, mc), block(rw_threads);
-        int rc2;
-        switch (rw_variant) {
-          case 1: rc2 = launch("hsmac_rw", k_hsmac_rw4_group<8, 3>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
-                               gx, gy, sc, hc, finalize, group_end); break;
-          case 2: rc2 = launch("hsmac_rw", k_hsmac_rw4_group<5, 3>, grid, block, rw_smem, ga, g, set, D, out, gb, xo,
-                               gx, gy, sc, hc, finalize, group_end); break;
-          default: rc2 = launch("hsmac_rw", k_hsmac_rw4_group<13, 3>, grid, block, rw_smem, ga, g, set, D, out, gb,
-                                xo, gx, gy, sc, hc, finalize, group_end);
-        }
-        LCS_TRY(rc2);
-      }
-      return LCS_OK;
-    }
-    const dim3 grid(sc.nitems), block(rw_threads);
-    float* Pf = (float*)P;
-    switch (rw_variant) {
-      case 1: return launch("hsmac_rw", k_hsmac_rw4<8, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw4, Pf, D, out,
-                            gb, xo, gx, gy, sc, hc, part, finalize, group_end);
-      case 2: return launch("hsmac_rw", k_hsmac_rw4<5, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw4, Pf, D, out,
-                            gb, xo, gx, gy, sc, hc, part, finalize, group_end);
-      default: return launch("hsmac_rw", k_hsmac_rw4<13, 3>, grid, block, rw_smem, dctx, g, set, tmaps_rw4, Pf, D,
-                             out, gb, xo, gx, gy, sc, hc, part, finalize, group_end);
     }
   }
   // the same sweep for every member of the group, kGroupMax members a launch
@@ -847,31 +699,6 @@ class Engine : public EngineBase {
     }
     return LCS_OK;
   }
-  int fused_tma(int set, Box D, Box out, int fill_r, double* part, int finalize, int group_end, int* nblocks) {
-    if (use_rw) return fused_rw(set, D, out, fill_r, part, finalize, group_end, nblocks);
-    if (!std::is_same<T, double>::value) return fail(LCS_EINVAL, "the thread-per-item TMA sweep is FP64 only");
-    if (fill_r > 0) LCS_TRY(fill(set, false, fill_r, 1));
-    const Box gb = bbox(out, cube(g, 1, 0));
-    const int xo = (gb.lo[0] & 1) ? gb.lo[0] : gb.lo[0] - 1;
-    const int gx = (gb.hi[0] - xo + 1 + TTX - 1) / TTX, gy = (gb.len(1) + TTY - 1) / TTY;
-    const int nzc = gb.len(2), ncols = gx * gy;
-    const int zc = pick_zchunk(nzc, ncols, num_sms * tma_ctas_per_sm);
-    const int nitems = ncols * ((nzc + zc - 1) / zc);
-    if (nitems > plan.partials_cap / 2) return fail(LCS_EINVAL, "grid too large for the partials buffer");
-    if (nblocks) *nblocks = nitems;
-    const dim3 grid(nitems), block(tma_threads);
-    switch (tile_variant) {
-      case 1: return launch("hsmac_tma", k_hsmac_tma<32, 16, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
-                            (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
-      case 2: return launch("hsmac_tma", k_hsmac_tma<32, 8, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
-                            (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
-      case 3: return launch("hsmac_tma", k_hsmac_tma<64, 16, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
-                            (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
-      default: return launch("hsmac_tma", k_hsmac_tma<64, 8, TNS>, grid, block, tma_smem, dctx, g, set, tmaps,
-                             (double*)P, D, out, gb, xo, gx, gy, zc, nitems, hc, part, finalize, group_end);
-    }
-  }
-
   // in-place colour phases over a box (both colours), partial sums appended
   int phases(int set, Box b, double* part, int* used) {
     if (grp) return fail(LCS_EINVAL, "group sweeps need the cooperative face kernel");
@@ -2343,8 +2170,7 @@ int Engine<T>::group_create(EngineBase* const* members, int m, GroupBase** out) 
                       a.omega == b.omega && a.epsp == b.epsp && a.itrmin == b.itrmin && a.itrmax == b.itrmax;
     if (!same) return fail(LCS_EINVAL, "group members differ in shape or HSMAC settings");
     if (!e->use_rw) return fail(LCS_EINVAL, "group members need the row-warp sweep");
-    if (e->rw_variant != L->rw_variant || e->zchunk_force != L->zchunk_force || e->sm_share != L->sm_share ||
-        e->use_rw4 != L->use_rw4)
+    if (e->rw_variant != L->rw_variant || e->zchunk_force != L->zchunk_force || e->sm_share != L->sm_share)
       return fail(LCS_EINVAL, "group members differ in launch shapes");
     if (e->async_pending) return fail(LCS_ESTATE, "asynchronous steps are in flight on a member");
     if (e->face_grid <= 0) return fail(LCS_EINVAL, "group members need the cooperative face kernel");

@@ -1,6 +1,6 @@
 // lcs_hsmac_rw.cuh -- the fused red-black HSMAC sweep, one warp per tile row.
 //
-// Same computation as k_hsmac_fused and k_hsmac_tma (both colour phases of
+// Same computation as k_hsmac_fused (both colour phases of
 // the reference's `foraxes(...; coloring=RedBlackFast())` sweep over a box D,
 // hsmac.jl:1-35, ping-ponged so that one pass replaces the two in-place
 // launches, bit-identical to them), arranged so that almost everything stays
@@ -39,7 +39,7 @@
 
 #include <type_traits>
 
-#include "lcs_hsmac_tma.cuh"
+#include "lcs_tma.cuh"
 
 namespace lcs {
 namespace {
@@ -100,8 +100,8 @@ template <typename T> __device__ __forceinline__ void st2(T* p, T a, T b) {
 template <typename T> __device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
 template <typename T> __device__ __forceinline__ T shfl_down1(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
 
-// face_update of k_hsmac_tma for either field type: the contributions of the
-// two cells sharing a face in the order of the in-place sweep.
+// The velocity update of one face for either field type: the contributions
+// of the two cells sharing the face in the order of the in-place sweep.
 template <typename T>
 __device__ __forceinline__ T face_update_t(T val, bool lower_first, bool ma, T da, bool mb, T db, T dci) {
   const T ta = da * dci, tb = db * dci;
@@ -161,7 +161,7 @@ struct RwRowBits {
 // x0 (a tile's first output column) puts x0-2 on a 16-byte boundary (x0 odd
 // in FP64, x0 = 3 mod 4 in FP32): the TMA boxes start there and every pair
 // (x0-2+2l, x0-1+2l) is aligned to its own size.  Work items are
-// (z chunk, tile column), chunk major, as in k_hsmac_tma.
+// (z chunk, tile column), chunk major.
 // The sweep of one handle as block `bid` of `nb` (k_hsmac_rw: the launch's
 // own grid; k_hsmac_rw_group: one handle per blockIdx.y).
 template <typename T, int TY, int NS, int RW>

@@ -114,45 +114,29 @@ def test_fp32_ten_steps_close_to_fp64(forcing):
 @pytest.mark.parametrize("dims,tb,ov", [((64, 64, 64), True, True), ((64, 64, 64), False, False),
                                         ((200, 48, 40), True, True), ((136, 40, 24), False, True),
                                         ((40, 24, 32), True, False)])
-def test_fp32_quad_sweep_agrees_with_pair_sweep(dims, tb, ov, monkeypatch):
-    """The four-cells-per-lane FP32 sweep (LCS_B200_RW4=1; tiles 120 wide,
-    several tile columns and partial tiles on these grids) against the
-    two-cells-per-lane one (the default): the
-    same arithmetic per cell, contracted alike or not, so U, V, W agree to
-    2e-6 and P to 1e-3 after a couple of 12 sweeps (measured values printed)."""
+def test_fp32_two_row_warps_agree_with_one_row_warps(dims, tb, ov, monkeypatch):
+    """The FP32 default tiles (29 rows, two rows per warp: LCS_B200_RW=29)
+    against 13-row tiles of one row per warp, on grids with several tile
+    columns, partial tiles and few z planes: the same arithmetic per cell, so
+    U, V, W agree to 2e-6 and P to 1e-3 after a couple of 12 sweeps (measured
+    values printed)."""
     rng = np.random.default_rng(sum(dims))
     flow = [rng.standard_normal((dims[2], dims[1], dims[0])) * 0.5 for _ in range(3)] + \
         [rng.standard_normal((dims[2], dims[1], dims[0])) * 0.1]
     out = {}
-    for quad in ("1", "0"):
-        monkeypatch.setenv("LCS_B200_RW4", quad)
+    for rows in ("29", "13"):
+        monkeypatch.setenv("LCS_B200_RW", rows)
         e = Engine(fp32_cfg(dims=dims, mode=F.MODE_FLOW, time_blocking=tb, overlap=ov, itrmin=6, itrmax=12,
                             epsp=1e-12))
         e.upload_flow(*flow)
         lg = e.couple(2, 0.003)
-        out[quad] = (lg, e.download_flow())
+        out[rows] = (lg, e.download_flow())
         e.close()
-    (lq, fq), (lp, fpair) = out["1"], out["0"]
-    assert lq["sweeps"] == lp["sweeps"]
-    errs = [rel_l2(a, b) for a, b in zip(fq, fpair)]
-    same = [bool(np.array_equal(a, b)) for a, b in zip(fq, fpair)]
-    print("quad vs pair", errs, "bitwise", same)
+    (l2, f2), (l1, f1) = out["29"], out["13"]
+    assert l2["sweeps"] == l1["sweeps"]
+    errs = [rel_l2(a, b) for a, b in zip(f2, f1)]
+    same = [bool(np.array_equal(a, b)) for a, b in zip(f2, f1)]
+    print("29-row vs 13-row", errs, "bitwise", same)
     assert max(errs[:3]) <= 2e-6, errs
     assert errs[3] <= 1e-3, errs
-    assert abs(lq["div"] - lp["div"]) <= 1e-4 * abs(lp["div"])
-
-
-@pytest.mark.parametrize("variant", ["8", "5"])
-def test_fp32_quad_row_variants_agree(variant, monkeypatch):
-    U, V, W, P = inits.spectral_flow(96, seed=8)
-    out = []
-    monkeypatch.setenv("LCS_B200_RW4", "1")
-    for v in (variant, "13"):
-        monkeypatch.setenv("LCS_B200_RW", v)
-        e = Engine(fp32_cfg(96, mode=F.MODE_FLOW, itrmin=6, itrmax=9, epsp=1e-12))
-        e.upload_flow(U, V, W, P)
-        e.couple(2, 0.003)
-        out.append(e.download_flow())
-        e.close()
-    errs = [rel_l2(a, b) for a, b in zip(*out)]
-    assert max(errs[:3]) <= 2e-6 and errs[3] <= 1e-3, errs
+    assert abs(l2["div"] - l1["div"]) <= 1e-4 * abs(l1["div"])

@@ -64,11 +64,10 @@ def test_update_and_fused_rhs_update_bitwise(stage):
 VARIANTS = [(tb, ov) for tb in (True, False) for ov in (True, False)]
 
 
-@pytest.fixture(params=["rw", "tma", "plain"])
+@pytest.fixture(params=["rw", "plain"])
 def sweep(request, monkeypatch):
-    """The implementations of the fused red-black sweep: the row-warp one
-    (default for red-black-fast), the thread-per-item TMA one and the
-    plain-load one."""
+    """The implementations of the fused red-black sweep: the row-warp one fed
+    by TMA (default for red-black-fast) and the plain-load one."""
     monkeypatch.setenv("LCS_B200_FUSED_SWEEP", request.param)
     return request.param
 
@@ -113,13 +112,13 @@ def test_hsmac_long_runs_and_early_exit(tb, ov, n, epsp, sweep):
 
 
 @pytest.mark.parametrize("tb,ov", VARIANTS)
-def test_tma_sweeps_equal_plain_sweep_128(tb, ov, monkeypatch):
-    """At 128^3 (several tiles and z chunks per sweep) the two TMA-fed sweeps
-    and the plain-load sweep give identical fields."""
+def test_row_warp_sweep_equals_plain_sweep_128(tb, ov, monkeypatch):
+    """At 128^3 (several tiles and z chunks per sweep) the TMA-fed row-warp
+    sweep and the plain-load sweep give identical fields."""
     from lcs_b200 import inits
 
     out = []
-    for mode in ("rw", "tma", "plain"):
+    for mode in ("rw", "plain"):
         monkeypatch.setenv("LCS_B200_FUSED_SWEEP", mode)
         e = Engine(make_config(128, mode=F.MODE_FLOW, time_blocking=tb, overlap=ov, itrmin=6, itrmax=12,
                                epsp=1e-12))

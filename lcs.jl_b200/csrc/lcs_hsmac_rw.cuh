@@ -6,8 +6,10 @@
 // launches, bit-identical to them), arranged so that almost everything stays
 // in registers:
 //  - a CTA owns a tile of RW_TX x TY output cells of the x-y plane and streams
-//    along z through a chunk of planes; warp w owns the tile row y0-1+w
-//    (TY+3 rows: the rows of the tile, one below and two above);
+//    along z through a chunk of planes; the TY+3 rows (the rows of the tile,
+//    one below and two above) go to the warps RW at a time: warp w owns rows
+//    y0-1+RW*w .. y0-2+RW*(w+1) (one row per warp for the FP64 13-row tiles,
+//    two for the FP32 29-row tiles);
 //  - lane l owns the x-pair (x0-2+2l, x0-1+2l), aligned to the pair's size in
 //    HBM and in shared memory, so every shared-memory access is a vector of a
 //    pair (or one element of it);

@@ -395,3 +395,68 @@ def test_errors_are_reported_not_raised_across_the_abi():
         g.rhs(3)
     with pytest.raises(LCSError):
         g.prop_get(5, 0)
+
+
+NONCUBIC = [(40, 24, 32), (70, 34, 96), (96, 40, 18)]
+
+
+@pytest.mark.parametrize("tb,ov", VARIANTS)
+@pytest.mark.parametrize("dims", NONCUBIC)
+def test_hsmac_noncubic_bitwise(dims, tb, ov, sweep):
+    """Grids with a different size per axis (per-axis spacings; several tile
+    columns and rows, partial tiles, few z planes): the couple's fields are
+    bit-identical to the oracle's, itr is equal and the residual agrees to
+    1e-12."""
+    cfg = make_config(dims=dims, mode=F.MODE_FLOW, time_blocking=tb, overlap=ov, itrmin=6, itrmax=20, epsp=1e-12,
+                      Re=50.0)
+    g, o = pair(cfg)
+    rng = np.random.default_rng(sum(dims))
+    for f in (0, 1, 2, 6):
+        a = rng.standard_normal(g.interior_shape) * (0.1 if f == 6 else 0.5)
+        g.field_set(f, a)
+        o.field_set(f, a)
+    lg = g.couple(2, 0.004)
+    lo = o.couple(2, 0.004)
+    assert lg["itr"] == lo["itr"] and lg["sweeps"] == lo["sweeps"]
+    assert abs(lg["div"] - lo["div"]) <= 1e-12 * lo["div"]
+    same_fields(g, o, (0, 1, 2, 6))
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_ten_steps_noncubic_rel_l2(graphs):
+    """Ten full steps (linear-power forcing, two particle species) on a 48 x 32 x 40
+    grid: couple itr equal, dt to 1e-13, fields and particles to rel-L2 <= 1e-10."""
+    from lcs_b200 import inits
+
+    dims = (48, 32, 40)
+    cfg = make_config(dims=dims, forcing=F.FORCING_LINEAR_POWER, power=0.5, Re=100.0, itrmin=6, itrmax=40,
+                      epsp=1e-8 * 2 * math.pi / 48, graphs=int(graphs),
+                      species=[{"n": 2000, "density_ratio": 843.0}, {"n": 1000, "density_ratio": 843.0}])
+    g, o = pair(cfg)
+    rng = np.random.default_rng(5)
+    for f in (0, 1, 2):
+        a = rng.standard_normal(g.interior_shape) * 0.5
+        g.field_set(f, a)
+        o.field_set(f, a)
+    for s, npart in enumerate((2000, 1000)):
+        x, y, z = inits.random_positions(npart, 30 + s)
+        zero = np.zeros(npart)
+        for e in (g, o):
+            e.upload_particles(s, np.full(npart, 0.02 * (s + 1)), x, y, z, zero, zero, zero)
+            e.init_particle_velocity(s)
+    lo = []
+    for _ in range(10):
+        lo.append(o.evolve(o.timestep()))
+    if graphs:
+        lg = g.step(10)
+    else:
+        lg = [g.evolve(g.timestep()) for _ in range(10)]
+    for a, b in zip(lg, lo):
+        assert a["couple1"]["itr"] == b["couple1"]["itr"] and a["couple2"]["itr"] == b["couple2"]["itr"]
+        assert abs(a["dt"] - b["dt"]) <= 1e-13 * b["dt"]
+    for a, b in zip(g.download_flow(), o.download_flow()):
+        assert rel_l2(a, b) <= 1e-10
+    for s in (0, 1):
+        pg, po = g.download_particles(s), o.download_particles(s)
+        for k in ("x", "y", "z", "u", "v", "w"):
+            assert rel_l2(pg[k], po[k]) <= 1e-10

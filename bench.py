@@ -53,9 +53,10 @@ OTHER_WORKLOADS = ("batch64", "serve", "makeindex", "couple256")
 
 # DRAM bytes (read + write) per interior cell of one launch of the sweep
 # kernel, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum) of
-# a D2 sweep (box 0:n+2) at 256^3, one per precision: not measured in the run
-# that reports them.
-SWEEP_DRAM_BYTES_PER_CELL = {"fp64": 67.8, "fp32-mixed": 35.0}
+# a D2 sweep (box 0:n+2) at 256^3, one per precision and default tile shape
+# (FP64 13-row tiles, FP32 29-row tiles): not measured in the run that
+# reports them.
+SWEEP_DRAM_BYTES_PER_CELL = {"fp64": 67.8, "fp32-mixed": 35.5}
 SWEEP_KERNELS = ("hsmac_rw", "hsmac_fused")
 # FP64 operations per interior cell of one rhs!+update! launch (k_rhs, both
 # stages alike): smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on
